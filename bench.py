@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Benchmark: real-time split-step iterations/s of the GPE solver at 128x128x32.
+
+Workload (the reference README's full simulation): 128 x 128 x 32 grid,
+dx = dy = 120 nm, dz = 600 nm, Dy-164 (163.929 Da), n_atoms = 2e4, edd = 1.5,
+MULTIPLE_GAUSS with 2 maxima in a MEXICAN trap (dd = 1500 nm), 1000 imaginary-time
+iterations (untimed set-up), then the potential switches to MEXICAN_FREE and
+real-time split-step iterations are timed.  psi is complex64 on the device.
+
+One bench "step" is one reference checkpoint interval of the real-time loop:
+1000 real_time_iter iterations (src/solver/solver.cpp:72-97 prints the time per
+1000 iterations).  `value` is whole-job RT iterations/s with the state resident
+in HBM; `e2e` is the same through the C ABI with host buffers (psi and V copied
+in, psi copied out every step).  L2 is flushed (256 MiB write) between timed
+steps; within a step the ~35 MB state stays cache-resident, as it does in any
+run of this grid.
+
+`--impl reference` times the reference's own CPU implementation (its
+CpuGrossPitaevskiSolver + FFTW solvers compiled from source, with the FP64
+FFTW-API shim, oracle/_ref/libgpe_ref.so) on the same workload with all host
+threads.
+
+Multi-GPU (torchrun): one independent replica per GPU (the path does not shard),
+no data-path collective; NCCL only for the barrier and the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 128, 128, 32
+ITERS_PER_STEP = 1000
+METRIC = "split-step RT iterations/s at 128x128x32"
+UNIT = "iterations/s"
+
+
+def workload_json(calc: str = "FS") -> dict:
+    return {
+        "nx": NX, "ny": NY, "nz": NZ, "dx": 120.0, "dy": 120.0, "dz": 600.0, "m": 163.929,
+        "n_atoms": 2e4, "edd": 1.5, "dd": 1500.0, "omega_x": 60.0, "omega_y": 60.0,
+        "omega_z": 120.0, "calc_strategy": calc, "init_strategy": "MULTIPLE_GAUSS",
+        "initial_maximas": 2, "pote_strategy": "MEXICAN", "iter_imag": 1000, "iter_real": 10000,
+        "fftw_n_threads": os.cpu_count() or 4,
+    }
+
+
+def config_dict() -> dict:
+    return {
+        "workload": "real-time split-step, 128x128x32, MEXICAN_FREE after 1000 IT iterations from "
+                    "MULTIPLE_GAUSS(2) in MEXICAN(dd=1500 nm), Dy-164, n_atoms=2e4, edd=1.5",
+        "grid": [NX, NY, NZ],
+        "iterations_per_step": ITERS_PER_STEP,
+        "precision": "complex64 psi, FP32 FFT, FP64 reductions",
+        "l2": "flushed between timed steps (256 MiB write); state L2-resident within a step",
+        "parallelism": "replicas",
+    }
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def dist_init(ws, local):
+    import torch
+
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax.append(float(f[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the reference's own CPU code)
+# ---------------------------------------------------------------------------
+def reference_cpu_rate(budget_s: float, min_iters: int = 3, max_iters: int = 200) -> dict:
+    """RT iterations/s of the reference's CpuGrossPitaevskiSolver on the workload,
+    from the state after 2 IT iterations (a bounded sample of the full run)."""
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    cfg = O.default_config(nx=NX, ny=NY, nz=NZ, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
+                           pote_strategy="MEXICAN", fftw_n_threads=threads)
+    kind = "reference" if O.ref_available() else "port"
+    S = O.RefSolver(cfg) if kind == "reference" else O.OracleSolver(cfg)
+    S.imag_steps(2)
+    S.change_potential("MEXICAN_FREE")
+    S.real_steps(1, 0)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while n < max_iters and (n < min_iters or time.perf_counter() - t0 < budget_s):
+        S.real_steps(1, n + 1)
+        n += 1
+    dt = time.perf_counter() - t0
+    S.close()
+    return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{n} RT iterations at {NX}x{NY}x{NZ} after 2 IT iterations, "
+                      f"fftw_n_threads={threads} (FP64 FFTW-API shim; FFTW3 absent on this image)"}
+
+
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    cfg = O.default_config(nx=NX, ny=NY, nz=NZ, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
+                           pote_strategy="MEXICAN", fftw_n_threads=threads)
+    kind = "reference" if O.ref_available() else "port"
+    S = O.RefSolver(cfg) if kind == "reference" else O.OracleSolver(cfg)
+    S.imag_steps(2)
+    S.change_potential("MEXICAN_FREE")
+    per_step = args.ref_iters_per_step
+    it = 0
+    for _ in range(args.warmup):
+        S.real_steps(per_step, it)
+        it += per_step
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        S.real_steps(per_step, it)
+        it += per_step
+    dt = time.perf_counter() - t0
+    S.close()
+    value = args.steps * per_step / dt
+    sample = (f"{per_step} RT iterations per step at {NX}x{NY}x{NZ}, fftw_n_threads={threads} "
+              f"(FP64 FFTW-API shim; FFTW3 absent on this image)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (reference initializers, deterministic)", "config": config_dict(),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (a line `traffic_bytes_per_launch <kernel> <bytes>`), or None."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for f in sorted(os.listdir(pdir)):
+        if not f.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(pdir, f)):
+            parts = line.strip().strip("`").split()
+            if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
+                try:
+                    return float(parts[2])
+                except ValueError:
+                    pass
+    return None
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def run_our_arm(args):
+    import numpy as np
+    import torch
+
+    ws, rank, local = dist_env()
+    dist_init(ws, local)
+    torch.cuda.set_device(local)
+    import gpesolver_b200 as G
+    from gpesolver_b200 import capi
+
+    p = G.params_from_json(workload_json())
+    solver = G.B200GrossPitaevskiSolver(p, precision="c64", device=local)
+    stream = torch.cuda.Stream(device=local)
+    solver.set_stream(stream.cuda_stream)
+    V_free = G.potential(p, "MEXICAN_FREE")
+    solver.load_pote(G.potential(p))
+    solver.load_buffer(G.initial_psi(p))
+    solver.imag_steps(p.iter_imag)
+    solver.load_pote(V_free)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    it = 0
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            solver.real_steps(ITERS_PER_STEP, it)
+            it += ITERS_PER_STEP
+    stream.synchronize()
+
+    # ---- device-resident timing -------------------------------------------
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    launches0 = solver.launch_count()
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for e0, e1 in evs:
+                flush.zero_()
+                e0.record(stream)
+                solver.real_steps(ITERS_PER_STEP, it)
+                e1.record(stream)
+                it += ITERS_PER_STEP
+        stream.synchronize()
+    torch.cuda.synchronize()
+    barrier(ws)
+    launches = solver.launch_count() - launches0
+    t_ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    t_max = max_over_ranks(ws, t_ms)
+    total_iters = sum_over_ranks(ws, float(args.steps * ITERS_PER_STEP))
+    value = total_iters / (t_max / 1e3)
+    clocks = clk.summary()
+
+    # ---- end to end through the C ABI with host buffers ---------------------
+    psi_host = torch.empty(2 * p.n, dtype=torch.float64, pin_memory=True).numpy()
+    V_host = torch.empty(p.n, dtype=torch.float64, pin_memory=True).numpy()
+    V_host[:] = V_free
+    psi_host[:] = solver.export_data().reshape(-1).view(np.float64)
+    e2e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+    barrier(ws)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for e0, e1 in e2e_evs:
+            flush.zero_()
+            e0.record(stream)
+            solver.load_pote(V_host)
+            solver.load_buffer(psi_host)
+            solver.real_steps(ITERS_PER_STEP, it)
+            out = solver.export_data()
+            e1.record(stream)
+            psi_host[:] = out.reshape(-1).view(np.float64)
+            it += ITERS_PER_STEP
+    stream.synchronize()
+    barrier(ws)
+    e2e_ms = max_over_ranks(ws, sum(e0.elapsed_time(e1) for e0, e1 in e2e_evs))
+    e2e_value = total_iters / (e2e_ms / 1e3)
+
+    # ---- per-kernel roofline (kernels timed alone) ---------------------------
+    per_step_count = {"DIP_Z_FWD": 1, "DIP_Y_FWD": 1, "DIP_X": 1, "DIP_Y_INV": 1, "DIP_Z_INV": 1,
+                      "KIN_Z_FWD": 1, "KIN_Y_FWD": 1, "KIN_X": 1, "KIN_Y_INV": 1, "KIN_Z_INV": 1,
+                      "PHASE": 2}
+    L = capi.lib()
+    kt = {}
+    import ctypes
+
+    for idx, name in enumerate(capi.KERNELS):
+        if name not in per_step_count:
+            continue
+        ms, by = ctypes.c_double(), ctypes.c_double()
+        capi.check(L.gpe_time_kernel(solver.handle, idx, 200, ctypes.byref(ms), ctypes.byref(by)))
+        kt[name] = (ms.value, by.value, L.gpe_kernel_name(idx).decode())
+    dom = max(per_step_count, key=lambda k: per_step_count[k] * kt[k][0])
+    ms, by, kname = kt[dom]
+    peak, peak_kind = measured_peak()
+    achieved = by / (ms * 1e-3) / 1e9
+    F = 8.0 * p.n
+    R4 = 4.0 * p.n
+    I = 8.0 * NX * 2 * NY * (NZ + 1)
+    b_rt = 6 * F + 3 * R4 + 4 * I  # algorithmic bytes per RT iteration (fused schedule)
+    per_gpu_rate = args.steps * ITERS_PER_STEP / (t_ms / 1e3)
+    traffic = traffic_from_profiles(kname)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = reference_cpu_rate(args.cpu_budget)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+            "data": "synthetic (reference initializers, deterministic)", "config": config_dict(),
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": int(16 * p.n + 8 * p.n),
+                    "d2h_bytes_per_step": int(16 * p.n)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": by,
+                         "launch_ms": ms},
+            "roofline_step": {"algorithmic_bytes_per_iteration": b_rt,
+                              "achieved": b_rt * per_gpu_rate / 1e9, "peak": peak, "unit": "GB/s",
+                              "frac": b_rt * per_gpu_rate / 1e9 / peak},
+            "kernels_ms": {k: round(v[0], 5) for k, v in kt.items()},
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-iters-per-step", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,117 @@
+"""ctypes binding of the gpe_b200 C ABI (include/gpe_b200.h).
+
+The shared library is the in-tree ``gpesolver_b200/libgpe_b200.so``.  Loading
+fails loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpe_b200.so")
+
+GPE_OK = 0
+GPE_ERR_ARG = 1
+GPE_ERR_SIZE = 2
+GPE_ERR_CUDA = 3
+GPE_ERR_STATE = 4
+GPE_ERR_NUMERIC = 5
+GPE_ERR_NOMEM = 6
+
+GPE_PREC_C64 = 0
+GPE_PREC_C128 = 1
+
+ERR_NAMES = {1: "GPE_ERR_ARG", 2: "GPE_ERR_SIZE", 3: "GPE_ERR_CUDA", 4: "GPE_ERR_STATE",
+             5: "GPE_ERR_NUMERIC", 6: "GPE_ERR_NOMEM"}
+
+
+class GpeError(RuntimeError):
+    """A failed gpe_* call (the reference throws std::runtime_error in these places)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class gpe_params(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+        ("m", ctypes.c_double), ("n_atoms", ctypes.c_double),
+        ("add", ctypes.c_double), ("cdd", ctypes.c_double), ("ggp11", ctypes.c_double),
+        ("gamma", ctypes.c_double), ("w_15", ctypes.c_double),
+        ("real_time_dt", ctypes.c_double), ("imag_time_dt", ctypes.c_double),
+        ("const_edd", ctypes.c_int),
+        ("edd", ctypes.c_double), ("edd_start", ctypes.c_double), ("edd_stop", ctypes.c_double),
+        ("iter_real", ctypes.c_long),
+        ("precision", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_lib = None
+
+# Every entry point declared in include/gpe_b200.h: (name, restype, argtypes).
+SIGNATURES = [
+    ("gpe_last_error", ctypes.c_char_p, []),
+    ("gpe_abi_version", ctypes.c_int, []),
+    ("gpe_params_derive", ctypes.c_int, [ctypes.POINTER(gpe_params)]),
+    ("gpe_params_edd_at", ctypes.c_int, [ctypes.POINTER(gpe_params), ctypes.c_long, _dp]),
+    ("gpe_create", ctypes.c_int, [ctypes.POINTER(gpe_params), ctypes.POINTER(ctypes.c_void_p)]),
+    ("gpe_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpe_set_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("gpe_get_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("gpe_synchronize", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpe_load_psi", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
+    ("gpe_load_potential", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
+    ("gpe_export_psi", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
+    ("gpe_export_fi3d", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
+    ("gpe_calc_fi3d", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpe_imag_iter_linear_step", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpe_imag_iter_nonlinear_step", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpe_calc_norm", ctypes.c_int, [ctypes.c_void_p, _dp]),
+    ("gpe_normalize", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpe_real_fft_potential_half_step", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpe_real_fft_kinetic_step", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpe_calc_energy", ctypes.c_int, [ctypes.c_void_p, _dp]),
+    ("gpe_set_coeffs", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]),
+    ("gpe_imag_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
+    ("gpe_real_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, ctypes.c_long]),
+    ("gpe_launch_count", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    ("gpe_time_kernel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]),
+    ("gpe_kernel_name", ctypes.c_char_p, [ctypes.c_int]),
+]
+
+KERNELS = ["DIP_Z_FWD", "DIP_Y_FWD", "DIP_X", "DIP_Y_INV", "DIP_Z_INV", "KIN_Z_FWD", "KIN_Y_FWD",
+           "KIN_X", "KIN_Y_INV", "KIN_Z_INV", "PHASE", "IT_UPDATE"]
+
+
+def lib() -> ctypes.CDLL:
+    """Load libgpe_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m gpesolver_b200.build` "
+                "(the solver has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != GPE_OK:
+        raise GpeError(rc, lib().gpe_last_error().decode(errors="replace"))
+
+
+def dptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_dp)

@@ -1,0 +1,991 @@
+// gpe_b200: host runtime of the B200 GPE solver backend and its C ABI.
+//
+// One Solver<R> per handle owns the device fields, the FFT plans and tables, a
+// CUDA stream and a cache of instantiated CUDA graphs (one per chunk of fused
+// iterations).  All work is enqueued on the handle's stream; the host only
+// waits where the reference's interface returns a value (norm, energies,
+// exported fields).
+#include "../../include/gpe_b200.h"
+#include "kernels.cuh"
+#include "plan.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace gpe {
+
+// ---------------------------------------------------------------------------
+// Non-template kernels
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_norm_finalize(const double *__restrict__ partial, int nparts, double dV,
+                    double *__restrict__ norm_state, int *__restrict__ status) {
+    __shared__ double red[256];
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < nparts; t += blockDim.x)
+        acc += partial[t];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double x = red[0] * dV;
+        norm_state[0]  = x;
+        norm_state[1]  = x;
+        if (!(x > 0.0) || !isfinite(x))
+            status[0] = 1;
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    k_energy_finalize(const double *__restrict__ partial, int nparts, double *__restrict__ out) {
+    __shared__ double red[256];
+    for (int t = 0; t < 5; ++t) {
+        double acc = 0.0;
+        for (int b = threadIdx.x; b < nparts; b += blockDim.x)
+            acc += partial[(size_t)t * nparts + b];
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s)
+                red[threadIdx.x] += red[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            out[t] = red[0];
+        __syncthreads();
+    }
+}
+
+__global__ void k_advance(int *counter, int by) { counter[0] += by; }
+
+__global__ void k_set_f64(double *p, double v) { p[0] = v; }
+
+// ---------------------------------------------------------------------------
+// Error helpers
+// ---------------------------------------------------------------------------
+static thread_local std::string t_last_error;
+
+#define GPE_CUDA(call)                                                                             \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            throw Error(e_ == cudaErrorMemoryAllocation ? GPE_ERR_NOMEM : GPE_ERR_CUDA,            \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                      \
+    } while (0)
+
+template <class T> struct DevBuf {
+    T *p     = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        n = count;
+        GPE_CUDA(cudaMalloc(&p, sizeof(T) * (count ? count : 1)));
+        GPE_CUDA(cudaMemset(p, 0, sizeof(T) * (count ? count : 1)));
+    }
+    ~DevBuf() {
+        if (p)
+            cudaFree(p);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Solver interface (precision-erased)
+// ---------------------------------------------------------------------------
+class SolverBase {
+  public:
+    virtual ~SolverBase() = default;
+    virtual void set_stream(cudaStream_t s)                  = 0;
+    virtual cudaStream_t stream() const                      = 0;
+    virtual void load_psi(const double *psi)                 = 0;
+    virtual void load_potential(const double *V)             = 0;
+    virtual void export_psi(double *out)                     = 0;
+    virtual void export_fi3d(double *out)                    = 0;
+    virtual void calc_fi3d()                                 = 0;
+    virtual void imag_linear()                               = 0;
+    virtual void imag_nonlinear()                            = 0;
+    virtual double calc_norm()                               = 0;
+    virtual void normalize()                                 = 0;
+    virtual void potential_half_step()                       = 0;
+    virtual void kinetic_step()                              = 0;
+    virtual void energy(double *out6)                        = 0;
+    virtual void set_coeffs(double ggp11, double gamma)      = 0;
+    virtual void imag_steps(long k)                          = 0;
+    virtual void real_steps(long k, long first_iter)         = 0;
+    virtual long long launches() const                       = 0;
+    virtual void time_kernel(int which, int reps, double *ms, double *bytes) = 0;
+    virtual size_t n() const                                 = 0;
+};
+
+// update_edd (src/parameters/parameters.cpp:53-59), FP64, same expression order.
+static void edd_at(const gpe_params &p, long iter, double *edd, double *ggp11, double *gamma) {
+    const double e = p.edd_start + (p.edd_stop - p.edd_start) * (unsigned)iter /
+                                       (double)(size_t)p.iter_real;
+    const double a = p.add / e;
+    *edd           = e;
+    *ggp11         = 4 * M_PI * a / p.m;
+    *gamma         = 128. * std::sqrt(M_PI) * std::pow(a, 2.5) / 3. / p.m * (1. + 1.5 * std::pow(e, 2));
+}
+
+template <class R> class Solver final : public SolverBase {
+    using C = cplx<R>;
+
+    // A planned line transform plus its launch tile.
+    struct Line {
+        LinePlan plan{};
+        DevBuf<C> tw;
+        int TB = 1;
+        size_t smem() const { return 2 * sizeof(C) * (size_t)TB * plan.L; }
+    };
+
+  public:
+    explicit Solver(const gpe_params &p) : P(p) {
+        nx = p.nx;
+        ny = p.ny;
+        nz = p.nz;
+        if (nx < 1 || ny < 1 || nz < 1)
+            throw Error(GPE_ERR_ARG, "grid dimensions must be positive");
+        if (!(p.dx > 0 && p.dy > 0 && p.dz > 0 && p.m > 0))
+            throw Error(GPE_ERR_ARG, "grid spacings and mass must be positive");
+        if ((long long)nx * ny * nz > (1LL << 30))
+            throw Error(GPE_ERR_SIZE, "grid larger than 2^30 points");
+        N = (size_t)nx * ny * nz;
+        H = nz + 1;
+        GPE_CUDA(cudaSetDevice(p.device));
+        GPE_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+        GPE_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+        cur = own_stream;
+
+        plan_line(kz, nz, 16);
+        plan_line(ky, ny, 32);
+        plan_line(kx, nx, 32);
+        plan_line(dz, 2 * nz, 16);
+        plan_line(dy, 2 * ny, 32);
+        plan_line(dx, 2 * nx, 32);
+
+        psi.alloc(N);
+        psii.alloc(N);
+        bnd.alloc(N);
+        V.alloc(N);
+        phi.alloc(N);
+        A.alloc((size_t)nx * 2 * ny * H);
+        staging.alloc(2 * N);
+        norm_state.alloc(4);
+        status.alloc(4);
+        iter_zero.alloc(1);
+        iter_base.alloc(1);
+        cur_coef.alloc(1);
+        eout.alloc(8);
+
+        nblk_elem = 148 * 8;
+        partial.alloc(nblk_elem);
+        epartial.alloc(5 * (size_t)nblk_elem);
+
+        build_tables();
+        set_coeffs(p.ggp11, p.gamma);
+        set_divisor_one();
+        GPE_CUDA(cudaStreamSynchronize(cur));
+        set_smem_attrs();
+    }
+
+    ~Solver() override {
+        for (auto &kv : graphs)
+            cudaGraphExecDestroy(kv.second);
+        if (coef_host)
+            cudaFreeHost(coef_host);
+        if (coef_event)
+            cudaEventDestroy(coef_event);
+        cudaStreamSynchronize(cur);
+        cudaStreamDestroy(cap_stream);
+        cudaStreamDestroy(own_stream);
+    }
+
+    void set_stream(cudaStream_t s) override { cur = s ? s : own_stream; }
+    cudaStream_t stream() const override { return cur; }
+    long long launches() const override { return n_launch; }
+    size_t n() const override { return N; }
+
+    // ---- data in / out ----------------------------------------------------
+    void load_psi(const double *h) override {
+        GPE_CUDA(cudaMemcpyAsync(staging.p, h, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, cur));
+        launch(k_from_f64<R>, grid_elem(2 * N), 256, 0, cur, (const double *)staging.p,
+               reinterpret_cast<R *>(psi.p), 2 * N);
+        GPE_CUDA(cudaMemcpyAsync(psii.p, psi.p, sizeof(C) * N, cudaMemcpyDeviceToDevice, cur));
+        GPE_CUDA(cudaMemcpyAsync(bnd.p, psi.p, sizeof(C) * N, cudaMemcpyDeviceToDevice, cur));
+        // calc_norm + normalize: the normalisation is held as the lazy divisor.
+        enqueue_norm(cur, psi.p, /*set_divisor=*/true);
+        lazy = true;
+        check_status();
+    }
+
+    void load_potential(const double *h) override {
+        GPE_CUDA(cudaMemcpyAsync(staging.p, h, sizeof(double) * N, cudaMemcpyHostToDevice, cur));
+        launch(k_from_f64<R>, grid_elem(N), 256, 0, cur, (const double *)staging.p, V.p, N);
+        GPE_CUDA(cudaStreamSynchronize(cur));
+    }
+
+    void export_psi(double *h) override {
+        launch(k_to_f64<R>, grid_elem(2 * N), 256, 0, cur, reinterpret_cast<const R *>(psi.p),
+               staging.p, 2 * N, (const double *)(norm_state.p + 1), 1);
+        GPE_CUDA(cudaMemcpyAsync(h, staging.p, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost, cur));
+        GPE_CUDA(cudaStreamSynchronize(cur));
+    }
+
+    void export_fi3d(double *h) override {
+        launch(k_to_f64<R>, grid_elem(N), 256, 0, cur, (const R *)phi.p, staging.p, N,
+               (const double *)one_ptr(), 1);
+        GPE_CUDA(cudaMemcpyAsync(h, staging.p, sizeof(double) * N, cudaMemcpyDeviceToHost, cur));
+        GPE_CUDA(cudaStreamSynchronize(cur));
+    }
+
+    // ---- the reference's virtuals ------------------------------------------
+    void calc_fi3d() override { enqueue_dipolar(cur, psi.p); }
+
+    void imag_linear() override { enqueue_it_update(cur, psi.p, psii.p); }
+
+    void imag_nonlinear() override {
+        std::swap(psi.p, psii.p);
+        set_divisor_one();
+        lazy = false;
+    }
+
+    double calc_norm() override {
+        materialize();
+        enqueue_norm(cur, psi.p, /*set_divisor=*/false);
+        set_divisor_one();
+        double x = 0;
+        GPE_CUDA(cudaMemcpyAsync(&x, norm_state.p, sizeof(double), cudaMemcpyDeviceToHost, cur));
+        GPE_CUDA(cudaStreamSynchronize(cur));
+        check_status();
+        return x;
+    }
+
+    void normalize() override {
+        // psi /= sqrt(xnorma): held lazily as the divisor norm_state[1] = xnorma.
+        GPE_CUDA(cudaMemcpyAsync(norm_state.p + 1, norm_state.p, sizeof(double),
+                                 cudaMemcpyDeviceToDevice, cur));
+        lazy = true;
+    }
+
+    void potential_half_step() override {
+        materialize();
+        enqueue_phase(cur, cur_coef.p, iter_zero.p, 0);
+    }
+
+    void kinetic_step() override {
+        materialize();
+        enqueue_kinetic(cur);
+    }
+
+    void energy(double *out) override {
+        const int nb = nblk_elem;
+        launch(k_energy_partial<R>, nb, 256, 0, cur, (const C *)psi.p, (const R *)V.p,
+               (const R *)phi.p, (const double *)(norm_state.p + 1), 1, epartial.p, nx, ny, nz,
+               1.0 / (P.dx * P.dx), 1.0 / (P.dy * P.dy), 1.0 / (P.dz * P.dz), ggp11_cur, P.cdd,
+               P.n_atoms, gamma_cur);
+        launch(k_energy_finalize, 1, 256, 0, cur, (const double *)epartial.p, nb, eout.p);
+        double e[5];
+        GPE_CUDA(cudaMemcpyAsync(e, eout.p, sizeof(e), cudaMemcpyDeviceToHost, cur));
+        GPE_CUDA(cudaStreamSynchronize(cur));
+        // Post-scaling of CpuGrossPitaevskiSolver::calc_energy (cpu_solver.cpp:185-191).
+        const double dV = P.dx * P.dy * P.dz, w = P.n_atoms;
+        out[0]          = e[0] * (dV / (2 * P.m) * w);
+        out[1]          = e[1] * (dV * w);
+        out[2]          = e[2] * (dV * std::pow(w, 2));
+        out[3]          = e[3] * dV;
+        out[4]          = e[4] * (dV * std::pow(w, 2.5));
+        out[5]          = out[0] + out[1] + out[2] + out[3] + out[4];
+        for (int t = 0; t < 6; ++t)
+            if (!std::isfinite(out[t]))
+                throw Error(GPE_ERR_NUMERIC, "non-finite energy");
+    }
+
+    void set_coeffs(double ggp11, double gamma) override {
+        ggp11_cur = ggp11;
+        gamma_cur = gamma;
+        StepCoef c{(ggp11 - P.cdd / 3) * P.n_atoms, gamma * P.w_15};
+        host_coef = c;
+        GPE_CUDA(cudaMemcpyAsync(cur_coef.p, &host_coef, sizeof(StepCoef), cudaMemcpyHostToDevice, cur));
+        GPE_CUDA(cudaStreamSynchronize(cur));
+    }
+
+    // ---- fused iterations ---------------------------------------------------
+    void imag_steps(long k) override {
+        if (k <= 0)
+            return;
+        if (!lazy)
+            set_divisor_one();
+        const int CH = kItChunk;
+        long done    = 0;
+        while (k - done >= CH) {
+            run_graph(0, CH);
+            done += CH;
+        }
+        if (k - done > 0)
+            run_graph(0, (int)(k - done));
+        lazy = true;
+        check_status();
+    }
+
+    void real_steps(long k, long first_iter) override {
+        if (k <= 0)
+            return;
+        materialize();
+        // Per-iteration coefficients (update_edd when ramping), FP64 on the host.
+        ensure_coef_capacity(k);
+        if (coef_event)
+            GPE_CUDA(cudaEventSynchronize(coef_event));
+        for (long t = 0; t < k; ++t) {
+            double g = ggp11_cur, gm = gamma_cur;
+            if (!P.const_edd) {
+                double e;
+                edd_at(P, first_iter + t, &e, &g, &gm);
+            }
+            coef_host[t] = StepCoef{(g - P.cdd / 3) * P.n_atoms, gm * P.w_15};
+            if (t == k - 1 && !P.const_edd)
+                set_coeffs(g, gm);
+        }
+        GPE_CUDA(cudaMemcpyAsync(coef_dev.p, coef_host, sizeof(StepCoef) * k, cudaMemcpyHostToDevice, cur));
+        GPE_CUDA(cudaEventRecord(coef_event, cur));
+        GPE_CUDA(cudaMemsetAsync(iter_base.p, 0, sizeof(int), cur));
+        const int CH = kRtChunk;
+        long done    = 0;
+        while (k - done >= CH) {
+            run_graph(1, CH);
+            done += CH;
+        }
+        if (k - done > 0)
+            run_graph(1, (int)(k - done));
+        check_status();
+    }
+
+    void time_kernel(int which, int reps, double *ms, double *bytes) override {
+        if (which < 0 || which >= GPE_K_COUNT || reps < 1)
+            throw Error(GPE_ERR_ARG, "bad kernel id or repetition count");
+        materialize();
+        // save the state the kernels modify
+        DevBuf<C> save_psi, save_A;
+        save_psi.alloc(N);
+        save_A.alloc(A.n);
+        GPE_CUDA(cudaMemcpyAsync(save_psi.p, psi.p, sizeof(C) * N, cudaMemcpyDeviceToDevice, cur));
+        GPE_CUDA(cudaMemcpyAsync(save_A.p, A.p, sizeof(C) * A.n, cudaMemcpyDeviceToDevice, cur));
+        cudaEvent_t e0, e1;
+        GPE_CUDA(cudaEventCreate(&e0));
+        GPE_CUDA(cudaEventCreate(&e1));
+        const double F = (double)sizeof(C) * N, Rb = (double)sizeof(R) * N;
+        const double I = (double)sizeof(C) * nx * 2 * ny * H, half = (double)sizeof(C) * nx * ny * H;
+        double b = 0;
+        auto one = [&]() {
+            const int lines = nx * ny;
+            switch (which) {
+            case GPE_K_DIP_Z_FWD:
+                launch(k_dip_z_fwd<R>, (lines + dz.TB - 1) / dz.TB, 256, dz.smem(), cur, (const C *)psi.p,
+                       (const double *)(norm_state.p + 1), 1, A.p, nx, ny, nz, (R)P.n_atoms, dz.plan, dz.TB);
+                b = F + half;
+                break;
+            case GPE_K_DIP_Y_FWD:
+                launch(k_dip_y<-1, R>, dim3((H + dy.TB - 1) / dy.TB, nx), 256, dy.smem(), cur, A.p, ny, H,
+                       ny, 2 * ny, dy.plan, dy.TB);
+                b = half + I;
+                break;
+            case GPE_K_DIP_X:
+                launch(k_dip_x<R>, (2 * ny * H + dx.TB - 1) / dx.TB, 256, dx.smem(), cur, A.p,
+                       (const R *)vk.p, nx, ny, H, (R)1, dx.plan, dx.TB);
+                b = 2 * I;
+                break;
+            case GPE_K_DIP_Y_INV:
+                launch(k_dip_y<+1, R>, dim3((H + dy.TB - 1) / dy.TB, nx), 256, dy.smem(), cur, A.p, ny, H,
+                       2 * ny, ny, dy.plan, dy.TB);
+                b = I + half;
+                break;
+            case GPE_K_DIP_Z_INV:
+                launch(k_dip_z_inv<R>, (lines + dz.TB - 1) / dz.TB, 256, dz.smem(), cur, (const C *)A.p, phi.p,
+                       nx, ny, nz, (R)(1.0 / (8.0 * (double)N)), dz.plan, dz.TB);
+                b = half + Rb;
+                break;
+            case GPE_K_KIN_Z_FWD:
+            case GPE_K_KIN_Z_INV:
+                if (which == GPE_K_KIN_Z_FWD)
+                    launch(k_kin_z<-1, R>, (lines + kz.TB - 1) / kz.TB, 256, kz.smem(), cur, psi.p, lines, nz,
+                           kz.plan, kz.TB);
+                else
+                    launch(k_kin_z<+1, R>, (lines + kz.TB - 1) / kz.TB, 256, kz.smem(), cur, psi.p, lines, nz,
+                           kz.plan, kz.TB);
+                b = 2 * F;
+                break;
+            case GPE_K_KIN_Y_FWD:
+            case GPE_K_KIN_Y_INV:
+                if (which == GPE_K_KIN_Y_FWD)
+                    launch(k_kin_y<-1, R>, dim3((nz + ky.TB - 1) / ky.TB, nx), 256, ky.smem(), cur, psi.p, ny,
+                           nz, ky.plan, ky.TB);
+                else
+                    launch(k_kin_y<+1, R>, dim3((nz + ky.TB - 1) / ky.TB, nx), 256, ky.smem(), cur, psi.p, ny,
+                           nz, ky.plan, ky.TB);
+                b = 2 * F;
+                break;
+            case GPE_K_KIN_X:
+                launch(k_kin_x<R>, (ny * nz + kx.TB - 1) / kx.TB, 256, kx.smem(), cur, psi.p,
+                       (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, nx, ny, nz, kx.plan, kx.TB);
+                b = 2 * F;
+                break;
+            case GPE_K_PHASE:
+                enqueue_phase(cur, cur_coef.p, iter_zero.p, 0);
+                b = 2 * F + 2 * Rb;
+                break;
+            default:
+                enqueue_it_update(cur, psi.p, psii.p);
+                b = 2 * F + 2 * Rb;
+                break;
+            }
+        };
+        one(); // warm-up
+        GPE_CUDA(cudaEventRecord(e0, cur));
+        for (int r = 0; r < reps; ++r)
+            one();
+        GPE_CUDA(cudaEventRecord(e1, cur));
+        GPE_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        GPE_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        GPE_CUDA(cudaMemcpyAsync(psi.p, save_psi.p, sizeof(C) * N, cudaMemcpyDeviceToDevice, cur));
+        GPE_CUDA(cudaMemcpyAsync(A.p, save_A.p, sizeof(C) * A.n, cudaMemcpyDeviceToDevice, cur));
+        GPE_CUDA(cudaStreamSynchronize(cur));
+        *ms    = (double)t / reps;
+        *bytes = b;
+    }
+
+  private:
+    static constexpr int kItChunk = 64;
+    static constexpr int kRtChunk = 32;
+
+    gpe_params P;
+    int nx, ny, nz, H;
+    size_t N;
+    Line kz, ky, kx, dz, dy, dx;
+    DevBuf<C> psi, psii, bnd, A, ex, ey, ez;
+    DevBuf<R> V, phi, vk;
+    DevBuf<double> staging, norm_state, partial, epartial, eout;
+    DevBuf<int> status, iter_zero, iter_base;
+    DevBuf<StepCoef> cur_coef, coef_dev;
+    StepCoef host_coef{};
+    StepCoef *coef_host   = nullptr;
+    size_t coef_cap       = 0;
+    cudaEvent_t coef_event = nullptr;
+    DevBuf<double> one_buf;
+    cudaStream_t own_stream = nullptr, cap_stream = nullptr, cur = nullptr;
+    std::map<std::tuple<int, int, const void *>, cudaGraphExec_t> graphs;
+    std::map<std::tuple<int, int, const void *>, int> graph_nodes;
+    int nblk_elem = 0;
+    bool lazy     = false;
+    double ggp11_cur = 0, gamma_cur = 0;
+    long long n_launch = 0;
+
+    int grid_elem(size_t n) const {
+        size_t b = (n + 255) / 256;
+        return (int)std::min<size_t>(b, (size_t)nblk_elem);
+    }
+
+    template <class K, class... Args>
+    void launch(K kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+        kernel<<<grid, block, smem, s>>>(args...);
+        GPE_CUDA(cudaGetLastError());
+        ++n_launch;
+    }
+
+    void plan_line(Line &ln, int L, int tbmax) {
+        std::vector<int> r = factor_line(L);
+        ln.plan.L          = L;
+        ln.plan.nstages    = (int)r.size();
+        for (size_t s = 0; s < r.size(); ++s)
+            ln.plan.radix[s] = r[s];
+        std::vector<double> t = twiddles(L);
+        std::vector<C> tc(L);
+        for (int m = 0; m < L; ++m)
+            tc[m] = C{(R)t[2 * m], (R)t[2 * m + 1]};
+        ln.tw.alloc(L);
+        GPE_CUDA(cudaMemcpy(ln.tw.p, tc.data(), sizeof(C) * L, cudaMemcpyHostToDevice));
+        ln.plan.tw = ln.tw.p;
+        // Tile: two Stockham buffers of TB lines within a 64 KiB budget per CTA.
+        const size_t budget = 64 * 1024;
+        int TB              = tbmax;
+        while (TB > 1 && 2 * sizeof(C) * (size_t)TB * L > budget)
+            TB >>= 1;
+        if (2 * sizeof(C) * (size_t)TB * L > 200 * 1024)
+            throw Error(GPE_ERR_SIZE, "FFT line of length " + std::to_string(L) + " too long");
+        ln.TB = TB;
+    }
+
+    void set_smem_attrs() {
+        auto set = [](const void *f, size_t bytes) {
+            if (bytes > 48 * 1024)
+                GPE_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        };
+        set((const void *)k_dip_z_fwd<R>, dz.smem());
+        set((const void *)k_dip_y<-1, R>, dy.smem());
+        set((const void *)k_dip_y<+1, R>, dy.smem());
+        set((const void *)k_dip_x<R>, dx.smem());
+        set((const void *)k_dip_z_inv<R>, dz.smem());
+        set((const void *)k_kin_z<-1, R>, kz.smem());
+        set((const void *)k_kin_z<+1, R>, kz.smem());
+        set((const void *)k_kin_y<-1, R>, ky.smem());
+        set((const void *)k_kin_y<+1, R>, ky.smem());
+        set((const void *)k_kin_x<R>, kx.smem());
+    }
+
+    // FP64 tables: V_dd(k) (fftw_poisson_solver.cpp:12-49) reduced by |kx|,|ky|
+    // symmetry, and the separable kinetic phase (fftw_split_solver.cpp:11-42).
+    void build_tables() {
+        {
+            const int px = 2 * nx, py = 2 * ny, pz = 2 * nz;
+            const double dkx = 2. * M_PI / (px * P.dx);
+            const double dky = 2. * M_PI / (py * P.dy);
+            const double dkz = 2. * M_PI / (pz * P.dz);
+            std::vector<R> t((size_t)(nx + 1) * (ny + 1) * H);
+            for (int i = 0; i <= nx; ++i) {
+                const double kxv = (i <= (px / 2)) ? i * dkx : (i - px) * dkx;
+                for (int j = 0; j <= ny; ++j) {
+                    const double kyv = (j <= (py / 2)) ? j * dky : (j - py) * dky;
+                    for (int k = 0; k < H; ++k) {
+                        const double kzv = (k <= (pz / 2)) ? k * dkz : (k - pz) * dkz;
+                        const double k2  = kxv * kxv + kyv * kyv + kzv * kzv;
+                        const double v   = (k2 > 1e-30) ? (kzv * kzv / k2) : 0.0;
+                        t[((size_t)i * (ny + 1) + j) * H + k] = (R)v;
+                    }
+                }
+            }
+            vk.alloc(t.size());
+            GPE_CUDA(cudaMemcpy(vk.p, t.data(), sizeof(R) * t.size(), cudaMemcpyHostToDevice));
+        }
+        {
+            const double dt = P.real_time_dt, fac = -dt / (2.0 * P.m);
+            auto axis = [&](int n, double d, double scale, DevBuf<C> &out) {
+                std::vector<C> t(n);
+                for (int i = 0; i < n; ++i) {
+                    const double kv = (i <= n / 2) ? (2.0 * M_PI * i / (n * d))
+                                                   : (2.0 * M_PI * (i - n) / (n * d));
+                    const double f  = fac * (kv * kv);
+                    t[i]            = C{(R)(std::cos(f) * scale), (R)(std::sin(f) * scale)};
+                }
+                out.alloc(n);
+                GPE_CUDA(cudaMemcpy(out.p, t.data(), sizeof(C) * n, cudaMemcpyHostToDevice));
+            };
+            axis(nx, P.dx, 1.0 / (double)N, ex);
+            axis(ny, P.dy, 1.0, ey);
+            axis(nz, P.dz, 1.0, ez);
+        }
+        one_buf.alloc(1);
+        const double one = 1.0;
+        GPE_CUDA(cudaMemcpy(one_buf.p, &one, sizeof(double), cudaMemcpyHostToDevice));
+    }
+
+    const double *one_ptr() const { return one_buf.p; }
+
+    void set_divisor_one() {
+        GPE_CUDA(cudaMemcpyAsync(norm_state.p + 1, one_buf.p, sizeof(double), cudaMemcpyDeviceToDevice, cur));
+    }
+
+    void materialize() {
+        if (!lazy)
+            return;
+        launch(k_scale<R>, grid_elem(N), 256, 0, cur, psi.p, N, (const double *)(norm_state.p + 1));
+        set_divisor_one();
+        lazy = false;
+    }
+
+    void check_status() {
+        int st = 0;
+        GPE_CUDA(cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, cur));
+        GPE_CUDA(cudaStreamSynchronize(cur));
+        if (st != 0) {
+            GPE_CUDA(cudaMemset(status.p, 0, sizeof(int)));
+            throw Error(GPE_ERR_NUMERIC, "non-finite or non-positive norm of psi");
+        }
+    }
+
+    void ensure_coef_capacity(long k) {
+        if ((size_t)k <= coef_cap)
+            return;
+        if (coef_event)
+            GPE_CUDA(cudaEventSynchronize(coef_event));
+        if (coef_host)
+            cudaFreeHost(coef_host);
+        size_t cap = std::max<size_t>((size_t)k, 1024);
+        GPE_CUDA(cudaMallocHost(&coef_host, sizeof(StepCoef) * cap));
+        coef_dev.~DevBuf();
+        new (&coef_dev) DevBuf<StepCoef>();
+        coef_dev.alloc(cap);
+        coef_cap = cap;
+        if (!coef_event)
+            GPE_CUDA(cudaEventCreateWithFlags(&coef_event, cudaEventDisableTiming));
+        // cached RT graphs point at the old coefficient buffer
+        for (auto it = graphs.begin(); it != graphs.end();) {
+            if (std::get<0>(it->first) == 1) {
+                cudaGraphExecDestroy(it->second);
+                graph_nodes.erase(it->first);
+                it = graphs.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
+
+    // ---- enqueue helpers (usable while capturing) ---------------------------
+    void enqueue_norm(cudaStream_t s, const C *p, bool set_divisor) {
+        launch(k_norm_partial<R>, nblk_elem, 256, 0, s, p, N, partial.p);
+        launch(k_norm_finalize, 1, 256, 0, s, (const double *)partial.p, nblk_elem,
+               P.dx * P.dy * P.dz, norm_state.p, status.p);
+        if (!set_divisor)
+            return;
+    }
+
+    void enqueue_dipolar(cudaStream_t s, const C *p) {
+        const int lines = nx * ny;
+        launch(k_dip_z_fwd<R>, (lines + dz.TB - 1) / dz.TB, 256, dz.smem(), s, p,
+               (const double *)(norm_state.p + 1), 1, A.p, nx, ny, nz, (R)P.n_atoms, dz.plan, dz.TB);
+        launch(k_dip_y<-1, R>, dim3((H + dy.TB - 1) / dy.TB, nx), 256, dy.smem(), s, A.p, ny, H, ny,
+               2 * ny, dy.plan, dy.TB);
+        const int cols = 2 * ny * H;
+        launch(k_dip_x<R>, (cols + dx.TB - 1) / dx.TB, 256, dx.smem(), s, A.p, (const R *)vk.p, nx,
+               ny, H, (R)1, dx.plan, dx.TB);
+        launch(k_dip_y<+1, R>, dim3((H + dy.TB - 1) / dy.TB, nx), 256, dy.smem(), s, A.p, ny, H,
+               2 * ny, ny, dy.plan, dy.TB);
+        const R inv_n = (R)(1.0 / (8.0 * (double)N));
+        launch(k_dip_z_inv<R>, (lines + dz.TB - 1) / dz.TB, 256, dz.smem(), s, (const C *)A.p, phi.p,
+               nx, ny, nz, inv_n, dz.plan, dz.TB);
+    }
+
+    void enqueue_kinetic(cudaStream_t s) {
+        const int lines = nx * ny;
+        launch(k_kin_z<-1, R>, (lines + kz.TB - 1) / kz.TB, 256, kz.smem(), s, psi.p, lines, nz,
+               kz.plan, kz.TB);
+        launch(k_kin_y<-1, R>, dim3((nz + ky.TB - 1) / ky.TB, nx), 256, ky.smem(), s, psi.p, ny, nz,
+               ky.plan, ky.TB);
+        const int cols = ny * nz;
+        launch(k_kin_x<R>, (cols + kx.TB - 1) / kx.TB, 256, kx.smem(), s, psi.p, (const C *)ex.p,
+               (const C *)ey.p, (const C *)ez.p, nx, ny, nz, kx.plan, kx.TB);
+        launch(k_kin_y<+1, R>, dim3((nz + ky.TB - 1) / ky.TB, nx), 256, ky.smem(), s, psi.p, ny, nz,
+               ky.plan, ky.TB);
+        launch(k_kin_z<+1, R>, (lines + kz.TB - 1) / kz.TB, 256, kz.smem(), s, psi.p, lines, nz,
+               kz.plan, kz.TB);
+    }
+
+    void enqueue_phase(cudaStream_t s, const StepCoef *coef, const int *base, int local) {
+        launch(k_phase<R>, grid_elem(N), 256, 0, s, psi.p, (const R *)V.p, (const R *)phi.p, coef,
+               base, local, nx, ny, nz, (R)(P.real_time_dt / 2.), (R)P.cdd);
+    }
+
+    void enqueue_it_update(cudaStream_t s, const C *in, C *out) {
+        const double m = P.m;
+        launch(k_it_update<R>, nblk_elem, 256, 0, s, in, out, (const C *)bnd.p, (const R *)V.p,
+               (const R *)phi.p, (const double *)(norm_state.p + 1), (const StepCoef *)cur_coef.p,
+               partial.p, nx, ny, nz, (R)(-0.5 / (m * P.dx * P.dx)), (R)(0.5 / (m * P.dy * P.dy)),
+               (R)(0.5 / (m * P.dz * P.dz)), (R)P.imag_time_dt, (R)P.cdd);
+    }
+
+    // One fused imaginary-time iteration from psi `in` into `out`:
+    // calc_fi3d -> Euler update -> calc_norm (normalize held as the divisor).
+    void enqueue_it_step(cudaStream_t s, const C *in, C *out) {
+        enqueue_dipolar(s, in);
+        enqueue_it_update(s, in, out);
+        launch(k_norm_finalize, 1, 256, 0, s, (const double *)partial.p, nblk_elem,
+               P.dx * P.dy * P.dz, norm_state.p, status.p);
+    }
+
+    // One fused real-time iteration (real_time_iter) on psi in place.
+    void enqueue_rt_step(cudaStream_t s, int local) {
+        enqueue_phase(s, coef_dev.p, iter_base.p, local);
+        enqueue_dipolar(s, psi.p);
+        enqueue_kinetic(s);
+        enqueue_phase(s, coef_dev.p, iter_base.p, local);
+    }
+
+    // kind 0: `count` IT iterations; kind 1: `count` RT iterations.
+    void run_graph(int kind, int count) {
+        auto key = std::make_tuple(kind, count, (const void *)psi.p);
+        auto it  = graphs.find(key);
+        if (it == graphs.end()) {
+            const long long before = n_launch;
+            GPE_CUDA(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                if (kind == 0) {
+                    C *a = psi.p, *b = psii.p;
+                    for (int t = 0; t < count; ++t) {
+                        enqueue_it_step(cap_stream, a, b);
+                        std::swap(a, b);
+                    }
+                } else {
+                    for (int t = 0; t < count; ++t)
+                        enqueue_rt_step(cap_stream, t);
+                    launch(k_advance, 1, 1, 0, cap_stream, iter_base.p, count);
+                }
+            } catch (...) {
+                cudaGraph_t g;
+                cudaStreamEndCapture(cap_stream, &g);
+                if (g)
+                    cudaGraphDestroy(g);
+                throw;
+            }
+            cudaGraph_t g;
+            GPE_CUDA(cudaStreamEndCapture(cap_stream, &g));
+            cudaGraphExec_t ge;
+            GPE_CUDA(cudaGraphInstantiate(&ge, g, 0));
+            cudaGraphDestroy(g);
+            graphs[key]      = ge;
+            graph_nodes[key] = (int)(n_launch - before);
+            n_launch         = before;
+            it               = graphs.find(key);
+        }
+        GPE_CUDA(cudaGraphLaunch(it->second, cur));
+        n_launch += graph_nodes[key];
+        if (kind == 0 && (count & 1))
+            std::swap(psi.p, psii.p);
+    }
+};
+
+} // namespace gpe
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+struct gpe_handle {
+    std::unique_ptr<gpe::SolverBase> impl;
+    int device = 0;
+};
+
+namespace {
+
+template <class F> int guarded(F &&f) {
+    try {
+        f();
+        return GPE_OK;
+    } catch (const gpe::Error &e) {
+        gpe::t_last_error = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        gpe::t_last_error = e.what();
+        return GPE_ERR_CUDA;
+    }
+}
+
+int bad(const char *msg) {
+    gpe::t_last_error = msg;
+    return GPE_ERR_ARG;
+}
+
+#define GPE_HANDLE(h)                                                                              \
+    if (!(h) || !(h)->impl)                                                                        \
+        return bad("null handle");                                                                 \
+    if (cudaSetDevice((h)->device) != cudaSuccess)                                                 \
+        return bad("cudaSetDevice failed");
+
+} // namespace
+
+extern "C" {
+
+const char *gpe_last_error(void) { return gpe::t_last_error.c_str(); }
+int gpe_abi_version(void) { return GPE_B200_ABI_VERSION; }
+
+int gpe_params_derive(gpe_params *p) {
+    if (!p)
+        return bad("null params");
+    if (!(p->m > 0) || !(p->edd > 0))
+        return bad("mass and edd must be positive");
+    // PhysicalParameters::init_parameters (src/parameters/parameters.cpp:37-51).
+    p->add          = 131.;
+    p->cdd          = 12. * M_PI * p->add / p->m;
+    const double a  = p->add / p->edd;
+    p->ggp11        = 4. * M_PI * a / p->m;
+    p->gamma        = 128. * std::sqrt(M_PI) * std::pow(a, 2.5) / 3. / p->m * (1. + 1.5 * std::pow(p->edd, 2));
+    p->w_15         = std::pow(p->n_atoms, 1.5);
+    p->real_time_dt = 1.00e10;
+    p->imag_time_dt = 1.25e11;
+    return GPE_OK;
+}
+
+int gpe_params_edd_at(const gpe_params *p, long iter, double *out3) {
+    if (!p || !out3)
+        return bad("null argument");
+    if (p->iter_real <= 0)
+        return bad("iter_real must be positive for an edd ramp");
+    gpe::edd_at(*p, iter, &out3[0], &out3[1], &out3[2]);
+    return GPE_OK;
+}
+
+int gpe_create(const gpe_params *p, gpe_handle **out) {
+    if (!p || !out)
+        return bad("null argument");
+    *out = nullptr;
+    if (p->precision != GPE_PREC_C64 && p->precision != GPE_PREC_C128)
+        return bad("unknown precision");
+    if (!p->const_edd && p->iter_real <= 0)
+        return bad("iter_real must be positive when edd is ramped");
+    return guarded([&] {
+        auto h    = std::make_unique<gpe_handle>();
+        h->device = p->device;
+        if (p->precision == GPE_PREC_C64)
+            h->impl.reset(new gpe::Solver<float>(*p));
+        else
+            h->impl.reset(new gpe::Solver<double>(*p));
+        *out = h.release();
+    });
+}
+
+int gpe_destroy(gpe_handle *h) {
+    if (!h)
+        return GPE_OK;
+    cudaSetDevice(h->device);
+    delete h;
+    return GPE_OK;
+}
+
+int gpe_set_stream(gpe_handle *h, void *s) {
+    GPE_HANDLE(h);
+    return guarded([&] { h->impl->set_stream((cudaStream_t)s); });
+}
+
+int gpe_get_stream(gpe_handle *h, void **s) {
+    GPE_HANDLE(h);
+    if (!s)
+        return bad("null argument");
+    *s = (void *)h->impl->stream();
+    return GPE_OK;
+}
+
+int gpe_synchronize(gpe_handle *h) {
+    GPE_HANDLE(h);
+    return guarded([&] {
+        cudaError_t e = cudaStreamSynchronize(h->impl->stream());
+        if (e != cudaSuccess)
+            throw gpe::Error(GPE_ERR_CUDA, cudaGetErrorString(e));
+    });
+}
+
+int gpe_load_psi(gpe_handle *h, const double *psi, size_t n) {
+    GPE_HANDLE(h);
+    if (!psi || n != h->impl->n())
+        return bad("gpe_load_psi: null pointer or n != nx*ny*nz");
+    return guarded([&] { h->impl->load_psi(psi); });
+}
+
+int gpe_load_potential(gpe_handle *h, const double *V, size_t n) {
+    GPE_HANDLE(h);
+    if (!V || n != h->impl->n())
+        return bad("gpe_load_potential: null pointer or n != nx*ny*nz");
+    return guarded([&] { h->impl->load_potential(V); });
+}
+
+int gpe_export_psi(gpe_handle *h, double *psi, size_t n) {
+    GPE_HANDLE(h);
+    if (!psi || n != h->impl->n())
+        return bad("gpe_export_psi: null pointer or n != nx*ny*nz");
+    return guarded([&] { h->impl->export_psi(psi); });
+}
+
+int gpe_export_fi3d(gpe_handle *h, double *fi3d, size_t n) {
+    GPE_HANDLE(h);
+    if (!fi3d || n != h->impl->n())
+        return bad("gpe_export_fi3d: null pointer or n != nx*ny*nz");
+    return guarded([&] { h->impl->export_fi3d(fi3d); });
+}
+
+int gpe_calc_fi3d(gpe_handle *h) {
+    GPE_HANDLE(h);
+    return guarded([&] { h->impl->calc_fi3d(); });
+}
+
+int gpe_imag_iter_linear_step(gpe_handle *h) {
+    GPE_HANDLE(h);
+    return guarded([&] { h->impl->imag_linear(); });
+}
+
+int gpe_imag_iter_nonlinear_step(gpe_handle *h) {
+    GPE_HANDLE(h);
+    return guarded([&] { h->impl->imag_nonlinear(); });
+}
+
+int gpe_calc_norm(gpe_handle *h, double *x) {
+    GPE_HANDLE(h);
+    return guarded([&] {
+        double v = h->impl->calc_norm();
+        if (x)
+            *x = v;
+    });
+}
+
+int gpe_normalize(gpe_handle *h) {
+    GPE_HANDLE(h);
+    return guarded([&] { h->impl->normalize(); });
+}
+
+int gpe_real_fft_potential_half_step(gpe_handle *h) {
+    GPE_HANDLE(h);
+    return guarded([&] { h->impl->potential_half_step(); });
+}
+
+int gpe_real_fft_kinetic_step(gpe_handle *h) {
+    GPE_HANDLE(h);
+    return guarded([&] { h->impl->kinetic_step(); });
+}
+
+int gpe_calc_energy(gpe_handle *h, double *out6) {
+    GPE_HANDLE(h);
+    if (!out6)
+        return bad("null argument");
+    return guarded([&] { h->impl->energy(out6); });
+}
+
+int gpe_set_coeffs(gpe_handle *h, double ggp11, double gamma) {
+    GPE_HANDLE(h);
+    return guarded([&] { h->impl->set_coeffs(ggp11, gamma); });
+}
+
+int gpe_imag_steps(gpe_handle *h, long k) {
+    GPE_HANDLE(h);
+    if (k < 0)
+        return bad("negative iteration count");
+    return guarded([&] { h->impl->imag_steps(k); });
+}
+
+int gpe_real_steps(gpe_handle *h, long k, long first_iter) {
+    GPE_HANDLE(h);
+    if (k < 0 || first_iter < 0)
+        return bad("negative iteration count");
+    return guarded([&] { h->impl->real_steps(k, first_iter); });
+}
+
+int gpe_time_kernel(gpe_handle *h, int which, int reps, double *ms, double *bytes) {
+    GPE_HANDLE(h);
+    if (!ms || !bytes)
+        return bad("null argument");
+    return guarded([&] { h->impl->time_kernel(which, reps, ms, bytes); });
+}
+
+const char *gpe_kernel_name(int which) {
+    static const char *names[] = {"k_dip_z_fwd", "k_dip_y", "k_dip_x", "k_dip_y", "k_dip_z_inv",
+                                  "k_kin_z", "k_kin_y", "k_kin_x", "k_kin_y", "k_kin_z",
+                                  "k_phase", "k_it_update"};
+    if (which < 0 || which >= GPE_K_COUNT)
+        return "";
+    return names[which];
+}
+
+int gpe_launch_count(gpe_handle *h, long long *count) {
+    GPE_HANDLE(h);
+    if (!count)
+        return bad("null argument");
+    *count = h->impl->launches();
+    return GPE_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,226 @@
+"""The B200 backend behind GPESolver's solver interface, for Python callers.
+
+``B200GrossPitaevskiSolver`` exposes the members of the reference's
+AbstractGrossPitaevskiSolver (src/solver/solver.hpp:17-72) with the same names
+and meaning -- load_buffer / load_pote / export_data, the pure virtuals
+(calc_fi3d, imag_iter_linear_step, imag_iter_nonlinear_step, calc_norm,
+normalize, real_fft_potential_half_step, real_fft_kinetic_step, calc_energy),
+the iteration bodies imag_time_iter / real_time_iter and the solve() driver --
+on top of the C ABI in include/gpe_b200.h.  Errors raise GpeError (a
+RuntimeError), where the reference throws std::runtime_error.
+
+Every numerical operation runs in libgpe_b200.so on the GPU; this module only
+moves host buffers and sequences calls.
+"""
+from __future__ import annotations
+
+import ctypes
+from collections import namedtuple
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import capi
+from .params import PhysicalParameters
+
+BECEnergies = namedtuple("BECEnergies", "e_kin e_pot e_int e_ext e_bmf e_total")
+
+PRECISIONS = {"c64": capi.GPE_PREC_C64, "c128": capi.GPE_PREC_C128}
+
+
+def make_gpe_params(p: PhysicalParameters, precision: str = "c64", device: int = 0) -> capi.gpe_params:
+    """Fill the C ABI's gpe_params from the PhysicalParameters fields."""
+    g = capi.gpe_params()
+    g.nx, g.ny, g.nz = p.nx, p.ny, p.nz
+    g.dx, g.dy, g.dz = p.dx, p.dy, p.dz
+    g.m, g.n_atoms = p.m, p.n_atoms
+    g.add, g.cdd, g.ggp11, g.gamma, g.w_15 = p.add, p.cdd, p.ggp11, p.gamma, p.w_15
+    g.real_time_dt, g.imag_time_dt = p.real_time_dt, p.imag_time_dt
+    g.const_edd = 1 if p.const_edd else 0
+    g.edd, g.edd_start, g.edd_stop = p.edd, p.edd_start, p.edd_stop
+    g.iter_real = max(int(p.iter_real), 1)
+    g.precision = PRECISIONS[precision]
+    g.device = device
+    return g
+
+
+class B200GrossPitaevskiSolver:
+    def __init__(self, params: PhysicalParameters, precision: str = "c64", device: int = 0):
+        self.params = params
+        self.precision = precision
+        self._L = capi.lib()
+        self._gp = make_gpe_params(params, precision, device)
+        h = ctypes.c_void_p()
+        capi.check(self._L.gpe_create(ctypes.byref(self._gp), ctypes.byref(h)))
+        self._h = h
+        self.n = params.n
+        self.xnorma = 0.0
+        self.enes: list[BECEnergies] = []
+        self.ene: Optional[BECEnergies] = None
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._L.gpe_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr: int) -> None:
+        capi.check(self._L.gpe_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def synchronize(self) -> None:
+        capi.check(self._L.gpe_synchronize(self._h))
+
+    def launch_count(self) -> int:
+        c = ctypes.c_longlong()
+        capi.check(self._L.gpe_launch_count(self._h, ctypes.byref(c)))
+        return c.value
+
+    # -- data in / out (solver.cpp:118-131, gpu_solver.cpp:136-155) -------
+    def load_buffer(self, psi) -> None:
+        a = _as_c128_flat(psi, self.n)
+        capi.check(self._L.gpe_load_psi(self._h, capi.dptr(a), self.n))
+
+    def load_pote(self, V) -> None:
+        a = np.ascontiguousarray(np.asarray(V, dtype=np.float64).reshape(-1))
+        if a.size != self.n:
+            raise capi.GpeError(capi.GPE_ERR_ARG, "bad potential import")
+        capi.check(self._L.gpe_load_potential(self._h, capi.dptr(a), self.n))
+
+    def export_data(self) -> np.ndarray:
+        """psi as complex128 of shape (nx, ny, nz)."""
+        out = np.zeros(2 * self.n)
+        capi.check(self._L.gpe_export_psi(self._h, capi.dptr(out), self.n))
+        return out.view(np.complex128).reshape(self.params.shape)
+
+    def export_fi3d(self) -> np.ndarray:
+        out = np.zeros(self.n)
+        capi.check(self._L.gpe_export_fi3d(self._h, capi.dptr(out), self.n))
+        return out.reshape(self.params.shape)
+
+    # -- the pure virtuals (solver.hpp:55-66) -------------------------------
+    def calc_fi3d(self) -> None:
+        capi.check(self._L.gpe_calc_fi3d(self._h))
+
+    def imag_iter_linear_step(self) -> None:
+        capi.check(self._L.gpe_imag_iter_linear_step(self._h))
+
+    def imag_iter_nonlinear_step(self) -> None:
+        capi.check(self._L.gpe_imag_iter_nonlinear_step(self._h))
+
+    def calc_norm(self) -> float:
+        x = ctypes.c_double()
+        capi.check(self._L.gpe_calc_norm(self._h, ctypes.byref(x)))
+        self.xnorma = x.value
+        return self.xnorma
+
+    def normalize(self) -> None:
+        capi.check(self._L.gpe_normalize(self._h))
+
+    def real_fft_potential_half_step(self) -> None:
+        capi.check(self._L.gpe_real_fft_potential_half_step(self._h))
+
+    def real_fft_kinetic_step(self) -> None:
+        capi.check(self._L.gpe_real_fft_kinetic_step(self._h))
+
+    def calc_energy(self) -> BECEnergies:
+        out = np.zeros(6)
+        capi.check(self._L.gpe_calc_energy(self._h, capi.dptr(out)))
+        self.ene = BECEnergies(*out.tolist())
+        self.enes.append(self.ene)
+        return self.ene
+
+    def set_coeffs(self, ggp11: float, gamma: float) -> None:
+        capi.check(self._L.gpe_set_coeffs(self._h, ggp11, gamma))
+
+    # -- iteration bodies (solver.cpp:99-112) -------------------------------
+    def imag_time_iter(self) -> None:
+        """One iteration through the individual virtuals (one call per virtual)."""
+        self.calc_fi3d()
+        self.imag_iter_linear_step()
+        self.imag_iter_nonlinear_step()
+        self.calc_norm()
+        self.normalize()
+
+    def real_time_iter(self) -> None:
+        self.real_fft_potential_half_step()
+        self.calc_fi3d()
+        self.real_fft_kinetic_step()
+        self.real_fft_potential_half_step()
+
+    # -- fused iterations (CUDA-graph replays) ------------------------------
+    def imag_steps(self, k: int) -> None:
+        capi.check(self._L.gpe_imag_steps(self._h, int(k)))
+
+    def real_steps(self, k: int, first_iter: int = 0) -> None:
+        capi.check(self._L.gpe_real_steps(self._h, int(k), int(first_iter)))
+        if not self.params.const_edd and k > 0:
+            self.params.update_edd(first_iter + k - 1)
+
+    # -- driver (AbstractGrossPitaevskiSolver::solve, solver.cpp:25-97) -----
+    def solve(self, checkpoint: Optional[Callable[[str, int, np.ndarray], None]] = None,
+              request_free_potential: Optional[Callable[[], np.ndarray]] = None) -> None:
+        """Runs the configured strategy with the reference's cadence: energies
+        and checkpoints after iterations 0, 100, 200, ... (IT) and 0, 1000, ...
+        (RT); the FS strategy switches to the free potential in between."""
+        p = self.params
+
+        def imag_phase():
+            done = 0
+            total = p.iter_imag + 1
+            while done < total:
+                k = 1 if done == 0 else min(100, total - done)
+                self.imag_steps(k)
+                done += k
+                it = done - 1
+                if it % 100 == 0:
+                    if checkpoint:
+                        checkpoint("imag", it, self.export_data())
+                    self.calc_energy()
+
+        def real_phase():
+            done = 0
+            total = p.iter_real + 1
+            while done < total:
+                k = 1 if done == 0 else min(1000, total - done)
+                self.real_steps(k, done)
+                done += k
+                it = done - 1
+                if it % 1000 == 0:
+                    if checkpoint:
+                        checkpoint("real", it, self.export_data())
+                    self.calc_energy()
+
+        if p.calc_strategy in ("IT", "FS"):
+            imag_phase()
+        if p.calc_strategy == "FS":
+            if request_free_potential is not None:
+                self.load_pote(request_free_potential())
+        if p.calc_strategy in ("RT", "FS"):
+            real_phase()
+
+
+def _as_c128_flat(psi, n: int) -> np.ndarray:
+    a = np.asarray(psi)
+    if np.iscomplexobj(a):
+        a = np.ascontiguousarray(a.reshape(-1), dtype=np.complex128).view(np.float64)
+    else:
+        a = np.ascontiguousarray(a.reshape(-1), dtype=np.float64)
+    if a.size != 2 * n:
+        raise capi.GpeError(capi.GPE_ERR_ARG, "bad wavefunction import")
+    return a

@@ -1,0 +1,157 @@
+/*
+ * gpe_b200 -- B200-native backend for GPESolver's solver/ hot path.
+ *
+ * A C ABI (plain pointers and sizes) that a C++ adapter deriving from the
+ * reference's AbstractGrossPitaevskiSolver (src/solver/solver.hpp:17-72) binds
+ * one-to-one: every pure virtual of that class has an entry point here, plus
+ * fused multi-iteration entry points that run whole reference iterations on the
+ * device (CUDA-graph replays, no host round trip per iteration).
+ *
+ * Conventions kept from the reference:
+ *   - grid layout row-major idx = (i*ny + j)*nz + k, x slowest, z fastest
+ *     (src/utils/types/mat3d/stdmat3d.hpp:26-28);
+ *   - psi on the host is interleaved (re, im) FP64, i.e. std::complex<double>
+ *     (src/context/context.hpp:30-36); V and phi are FP64;
+ *   - all quantities in atomic units, as PhysicalParameters holds them
+ *     (src/parameters/parameters.hpp:10-123).
+ *
+ * Every call returns 0 on success or a GPE_ERR_* code; gpe_last_error() gives the
+ * message of the last failure on the calling thread.  One handle is used by one
+ * host thread at a time; distinct handles may be driven from distinct threads.
+ */
+#ifndef GPE_B200_H
+#define GPE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPE_B200_ABI_VERSION 1
+
+enum {
+    GPE_OK            = 0,
+    GPE_ERR_ARG       = 1, /* invalid argument (null pointer, size mismatch, bad value) */
+    GPE_ERR_SIZE      = 2, /* grid size the FFT planner does not support */
+    GPE_ERR_CUDA      = 3, /* CUDA runtime error (launch, copy, allocation) */
+    GPE_ERR_STATE     = 4, /* call not valid in the handle's current state */
+    GPE_ERR_NUMERIC   = 5, /* NaN/Inf detected in a reduction */
+    GPE_ERR_NOMEM     = 6  /* device allocation failed */
+};
+
+/* Arithmetic of the fields on the device. */
+enum {
+    GPE_PREC_C64  = 0, /* complex64 psi, FP32 FFT/stencil, FP64 reductions (default) */
+    GPE_PREC_C128 = 1  /* complex128 psi, FP64 everywhere (reference precision) */
+};
+
+/* The PhysicalParameters fields the solver backend reads
+ * (src/parameters/parameters.hpp:10-123), in atomic units. */
+typedef struct gpe_params {
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double m;
+    double n_atoms;
+    double add;            /* dipolar length, 131 a0 (parameters.cpp:43) */
+    double cdd;            /* 12 pi add / m */
+    double ggp11;          /* 4 pi a / m */
+    double gamma;          /* LHY coefficient */
+    double w_15;           /* n_atoms^1.5 */
+    double real_time_dt;   /* 1.00e10 (parameters.hpp:69-70) */
+    double imag_time_dt;   /* 1.25e11 (parameters.hpp:71-72) */
+    int const_edd;         /* 1: edd fixed; 0: RT ramps edd_start -> edd_stop */
+    double edd, edd_start, edd_stop;
+    long iter_real;        /* ramp length (update_edd divides by it) */
+    int precision;         /* GPE_PREC_* */
+    int device;            /* CUDA device ordinal */
+} gpe_params;
+
+typedef struct gpe_handle gpe_handle;
+
+const char *gpe_last_error(void);
+int gpe_abi_version(void);
+
+/* Fill the derived coefficients (add, cdd, ggp11, gamma, w_15) and the default
+ * time steps exactly as PhysicalParameters::init_parameters does
+ * (src/parameters/parameters.cpp:37-51, parameters.hpp:69-72).  Reads nx..edd. */
+int gpe_params_derive(gpe_params *p);
+
+/* Coefficients of PhysicalParameters::update_edd(iter) (parameters.cpp:53-59):
+ * out3 = {edd, ggp11, gamma}. */
+int gpe_params_edd_at(const gpe_params *p, long iter, double *out3);
+
+/* Lifecycle.  Replaces GpuGrossPitaevskiSolver's constructor, init_containers()
+ * and prepare_fft() (src/solver/cuda_solver/gpu_solver.cpp:4-38; solver.hpp:56,66):
+ * allocates the device fields, plans the FFTs and builds the dipolar kernel
+ * V_dd(k) and the kinetic phase tables in FP64. */
+int gpe_create(const gpe_params *p, gpe_handle **out);
+int gpe_destroy(gpe_handle *h);
+
+/* Run on a caller-provided cudaStream_t (NULL: the handle's own stream). */
+int gpe_set_stream(gpe_handle *h, void *cuda_stream);
+int gpe_get_stream(gpe_handle *h, void **cuda_stream);
+int gpe_synchronize(gpe_handle *h);
+
+/* --- data in / out (import_data, import_pote, export_data; solver.hpp:68-70) --- */
+
+/* AbstractGrossPitaevskiSolver::load_buffer (solver.cpp:118-125): psi and the
+ * scratch copy psii both take the given values, then calc_norm + normalize.
+ * n = nx*ny*nz complex values (2n doubles). */
+int gpe_load_psi(gpe_handle *h, const double *psi_c128, size_t n);
+/* load_pote (solver.cpp:127-131). n = nx*ny*nz doubles. */
+int gpe_load_potential(gpe_handle *h, const double *V, size_t n);
+/* export_data: the current psi (normalised if the last step was an imaginary-time
+ * step), widened to complex128. */
+int gpe_export_psi(gpe_handle *h, double *psi_c128, size_t n);
+/* The dipolar field fi3d as last computed (FP64 copy). */
+int gpe_export_fi3d(gpe_handle *h, double *fi3d, size_t n);
+
+/* --- the pure virtuals of AbstractGrossPitaevskiSolver (solver.hpp:55-66) --- */
+
+int gpe_calc_fi3d(gpe_handle *h);                 /* calc_fi3d (Poisson::execute) */
+int gpe_imag_iter_linear_step(gpe_handle *h);     /* fused Euler update into psii */
+int gpe_imag_iter_nonlinear_step(gpe_handle *h);  /* psi <- psii (nonlinear term is fused above) */
+int gpe_calc_norm(gpe_handle *h, double *xnorma); /* xnorma = sum |psi|^2 dV (FP64) */
+int gpe_normalize(gpe_handle *h);                 /* psi /= sqrt(xnorma) */
+int gpe_real_fft_potential_half_step(gpe_handle *h);
+int gpe_real_fft_kinetic_step(gpe_handle *h);
+/* calc_energy: out6 = {e_kin, e_pot, e_int, e_ext (dipolar), e_bmf, e_total}. */
+int gpe_calc_energy(gpe_handle *h, double *out6);
+/* Coefficients the nonlinear terms use from the next call on (update_edd). */
+int gpe_set_coeffs(gpe_handle *h, double ggp11, double gamma);
+
+/* --- fused iterations (the fast path) --- */
+
+/* k reference imaginary-time iterations (imag_time_iter, solver.cpp:99-105). */
+int gpe_imag_steps(gpe_handle *h, long k);
+/* k reference real-time iterations first_iter .. first_iter+k-1 (real_time_iter,
+ * solver.cpp:107-112), applying update_edd(iter) before each one when the
+ * handle's const_edd is 0 (calc_evolution, solver.cpp:75-77). */
+int gpe_real_steps(gpe_handle *h, long k, long first_iter);
+
+/* Number of kernels the library launched on this handle since creation. */
+int gpe_launch_count(gpe_handle *h, long long *count);
+
+/* --- measurement --- */
+
+/* Kernels of the real-time iteration, for per-kernel timing. */
+enum {
+    GPE_K_DIP_Z_FWD = 0, GPE_K_DIP_Y_FWD, GPE_K_DIP_X, GPE_K_DIP_Y_INV, GPE_K_DIP_Z_INV,
+    GPE_K_KIN_Z_FWD, GPE_K_KIN_Y_FWD, GPE_K_KIN_X, GPE_K_KIN_Y_INV, GPE_K_KIN_Z_INV,
+    GPE_K_PHASE, GPE_K_IT_UPDATE, GPE_K_COUNT
+};
+/* Launches kernel `which` `reps` times back to back on the handle's stream
+ * between two CUDA events and reports the mean time per launch and the
+ * kernel's algorithmic bytes per launch (compulsory reads + writes of its
+ * inputs and outputs).  The solver state is saved before and restored after. */
+int gpe_time_kernel(gpe_handle *h, int which, int reps, double *ms_per_launch,
+                    double *bytes_per_launch);
+/* Name of kernel `which` as it appears in a profiler's launch list. */
+const char *gpe_kernel_name(int which);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,191 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's golden
+fixtures and the FP64 oracle.
+
+Tolerances (relative L2 of psi / phi, relative error of energies):
+  * c128 (FP64 everywhere): 1e-11 -- rounding-level agreement;
+  * c64 (complex64 psi, FP32 FFT/stencil, FP64 reductions): 2e-5 for a few
+    iterations, the same bound that the 1e-5-after-10k-steps target implies per
+    call.
+"""
+import numpy as np
+import pytest
+
+import gpesolver_b200 as G
+from oracle import oracle as O
+
+from .helpers import c128, golden, golden_cases, gparams, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"c128": 1e-11, "c64": 2e-5}
+ETOL = {"c128": 1e-10, "c64": 2e-5}
+CASES = list(golden_cases().CASES)
+
+
+def _solver(name, prec):
+    over = golden_cases().CASES[name][0]
+    cfg = O.default_config(**over)
+    p = gparams(cfg)
+    return G.B200GrossPitaevskiSolver(p, precision=prec), cfg
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+@pytest.mark.parametrize("name", CASES)
+def test_single_operations_match_golden(name, prec):
+    g = golden(name)
+    s, _ = _solver(name, prec)
+    with s:
+        s.load_pote(g["pote0"])
+        s.load_buffer(g["psi0"])
+        assert rel_l2(s.export_data(), c128(g["psi0"])) < TOL[prec]
+        s.calc_fi3d()
+        assert rel_l2(s.export_fi3d(), g["op_fi3d"]) < TOL[prec]
+        s.real_fft_potential_half_step()
+        assert rel_l2(s.export_data(), c128(g["op_pot_half"])) < TOL[prec]
+        s.real_fft_kinetic_step()
+        assert rel_l2(s.export_data(), c128(g["op_kinetic"])) < TOL[prec]
+        e = np.array(s.calc_energy())
+        np.testing.assert_allclose(e, g["op_energy"], rtol=ETOL[prec], atol=1e-30 + ETOL[prec] * abs(g["op_energy"][5]))
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+@pytest.mark.parametrize("name", CASES)
+def test_fused_iterations_match_golden(name, prec):
+    g = golden(name)
+    _, n_it, switch, n_rt, first = golden_cases().CASES[name]
+    s, _ = _solver(name, prec)
+    with s:
+        s.load_pote(g["pote0"])
+        s.load_buffer(g["psi0"])
+        if n_it:
+            s.imag_steps(n_it)
+            assert rel_l2(s.export_data(), c128(g["it_psi"])) < TOL[prec]
+            assert rel_l2(s.export_fi3d(), g["it_fi3d"]) < TOL[prec]
+            e = np.array(s.calc_energy())
+            assert abs(e[5] - g["it_energy"][5]) < ETOL[prec] * abs(g["it_energy"][5])
+        if switch:
+            s.load_pote(g["pote1"])
+        s.real_steps(n_rt, first)
+        assert rel_l2(s.export_data(), c128(g["rt_psi"])) < TOL[prec]
+        assert rel_l2(s.export_fi3d(), g["rt_fi3d"]) < TOL[prec]
+        e = np.array(s.calc_energy())
+        assert abs(e[5] - g["rt_energy"][5]) < ETOL[prec] * abs(g["rt_energy"][5])
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_virtual_by_virtual_iterations_match_fused(prec):
+    cfg = O.default_config(nx=24, ny=20, nz=12, init_strategy="MULTIPLE_GAUSS", pote_strategy="MEXICAN")
+    p = gparams(cfg)
+    V, psi0 = G.potential(p), G.initial_psi(p)
+    outs = []
+    for fused in (True, False):
+        with G.B200GrossPitaevskiSolver(p, precision=prec) as s:
+            s.load_pote(V)
+            s.load_buffer(psi0)
+            if fused:
+                s.imag_steps(3)
+                s.real_steps(3, 0)
+            else:
+                for _ in range(3):
+                    s.imag_time_iter()
+                for _ in range(3):
+                    s.real_time_iter()
+            outs.append(s.export_data())
+    assert rel_l2(outs[0], outs[1]) < (1e-13 if prec == "c128" else 1e-6)
+
+
+@pytest.mark.parametrize("k", [1, 2, 63, 64, 65, 130])
+def test_chunk_boundaries_imag_and_real(k):
+    cfg = O.default_config(nx=32, ny=32, nz=16, init_strategy="GAUSS", pote_strategy="HARMONIC",
+                           edd=None, edd_start=1.3, edd_stop=1.6, iter_real=200)
+    p = gparams(cfg)
+    ref = O.OracleSolver(cfg)
+    ref.imag_steps(k)
+    ref.real_steps(k, 7)
+    with G.B200GrossPitaevskiSolver(p, precision="c128") as s:
+        s.load_pote(G.potential(p))
+        s.load_buffer(G.initial_psi(p))
+        s.imag_steps(k)
+        s.real_steps(k, 7)
+        got = s.export_data()
+    want = c128(ref.psi())
+    ref.close()
+    assert rel_l2(got, want) < 1e-10
+
+
+def test_readme_config_imaginary_time_c64():
+    # BASELINE config 1 geometry (64^2 x 16, HARMONIC, GAUSS), 200 IT iterations
+    cfg = O.default_config(nx=64, ny=64, nz=16, init_strategy="GAUSS", pote_strategy="HARMONIC")
+    p = gparams(cfg, "IT")
+    ref = O.OracleSolver(cfg)
+    ref.imag_steps(200)
+    with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
+        s.load_pote(G.potential(p))
+        s.load_buffer(G.initial_psi(p))
+        s.imag_steps(200)
+        got = s.export_data()
+        e = s.calc_energy()
+    want = c128(ref.psi())
+    e_ref = ref.energy()
+    ref.close()
+    assert rel_l2(got, want) < 1e-5
+    assert abs(e.e_total - e_ref[5]) < 1e-6 * abs(e_ref[5])
+
+
+def test_full_simulation_128_c64():
+    # BASELINE config 2 geometry (128^2 x 32, MEXICAN, 2 maxima), short FS run
+    cfg = O.default_config(nx=128, ny=128, nz=32, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
+                           pote_strategy="MEXICAN", fftw_n_threads=8)
+    p = gparams(cfg)
+    ref = O.OracleSolver(cfg)
+    ref.imag_steps(10)
+    ref.change_potential("MEXICAN_FREE")
+    ref.real_steps(10, 0)
+    with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
+        s.load_pote(G.potential(p))
+        s.load_buffer(G.initial_psi(p))
+        s.imag_steps(10)
+        s.load_pote(G.potential(p, "MEXICAN_FREE"))
+        s.real_steps(10, 0)
+        got = s.export_data()
+    want = c128(ref.psi())
+    ref.close()
+    assert rel_l2(got, want) < 2e-5
+
+
+def test_real_time_conserves_norm_at_256():
+    # BASELINE config 3 geometry (256^2 x 64, FREE, SETUP_GAUSS 3x3x2, edd ramp):
+    # size-independent property -- split-step RT is unitary, the norm stays 1.
+    cfg = O.default_config(nx=256, ny=256, nz=64, init_strategy="SETUP_GAUSS", bec_droplets_x=3,
+                           bec_droplets_y=3, bec_droplets_z=2, pote_strategy="FREE", edd=None,
+                           edd_start=1.40, edd_stop=1.60, iter_real=20000)
+    p = gparams(cfg, "RT")
+    with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
+        s.load_pote(G.potential(p))
+        s.load_buffer(G.initial_psi(p))
+        n0 = s.calc_norm()
+        s.real_steps(200, 0)
+        n1 = s.calc_norm()
+    assert abs(n0 - 1.0) < 1e-6
+    assert abs(n1 - n0) < 1e-5
+
+
+def test_nonfinite_state_is_reported():
+    cfg = O.default_config(nx=16, ny=16, nz=8)
+    p = gparams(cfg)
+    with G.B200GrossPitaevskiSolver(p) as s:
+        s.load_pote(G.potential(p))
+        with pytest.raises(G.GpeError):
+            s.load_buffer(np.zeros(2 * p.n))
+        bad = G.initial_psi(p)
+        bad[100] = np.nan
+        with pytest.raises(G.GpeError):
+            s.load_buffer(bad)
+
+
+def test_unsupported_grid_is_rejected():
+    cfg = O.default_config(nx=22, ny=16, nz=8)  # 22 = 2 * 11
+    p = gparams(cfg)
+    with pytest.raises(G.GpeError) as ei:
+        G.B200GrossPitaevskiSolver(p)
+    assert ei.value.code == 2
