@@ -66,6 +66,7 @@ SIGNATURES = [
     ("gpe_get_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     ("gpe_synchronize", ctypes.c_int, [ctypes.c_void_p]),
     ("gpe_load_psi", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
+    ("gpe_import_psi", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     ("gpe_load_potential", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     ("gpe_export_psi", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     ("gpe_export_fi3d", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),

@@ -108,13 +108,14 @@ class SolverBase {
     virtual void set_stream(cudaStream_t s)                  = 0;
     virtual cudaStream_t stream() const                      = 0;
     virtual void load_psi(const double *psi)                 = 0;
+    virtual void import_psi(const double *psi)               = 0;
     virtual void load_potential(const double *V)             = 0;
     virtual void export_psi(double *out)                     = 0;
     virtual void export_fi3d(double *out)                    = 0;
     virtual void calc_fi3d()                                 = 0;
     virtual void imag_linear()                               = 0;
     virtual void imag_nonlinear()                            = 0;
-    virtual double calc_norm()                               = 0;
+    virtual double calc_norm(bool to_host)                   = 0;
     virtual void normalize()                                 = 0;
     virtual void potential_half_step()                       = 0;
     virtual void kinetic_step()                              = 0;
@@ -228,6 +229,17 @@ template <class R> class Solver final : public SolverBase {
         check_status();
     }
 
+    void import_psi(const double *h) override {
+        GPE_CUDA(cudaMemcpyAsync(staging.p, h, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, cur));
+        launch(k_from_f64<R>, grid_elem(2 * N), 256, 0, cur, (const double *)staging.p,
+               reinterpret_cast<R *>(psi.p), 2 * N);
+        GPE_CUDA(cudaMemcpyAsync(psii.p, psi.p, sizeof(C) * N, cudaMemcpyDeviceToDevice, cur));
+        GPE_CUDA(cudaMemcpyAsync(bnd.p, psi.p, sizeof(C) * N, cudaMemcpyDeviceToDevice, cur));
+        set_divisor_one();
+        lazy = false;
+        GPE_CUDA(cudaStreamSynchronize(cur));
+    }
+
     void load_potential(const double *h) override {
         GPE_CUDA(cudaMemcpyAsync(staging.p, h, sizeof(double) * N, cudaMemcpyHostToDevice, cur));
         launch(k_from_f64<R>, grid_elem(N), 256, 0, cur, (const double *)staging.p, V.p, N);
@@ -259,14 +271,19 @@ template <class R> class Solver final : public SolverBase {
         lazy = false;
     }
 
-    double calc_norm() override {
+    // Reference semantics: no error on a zero or non-finite norm here (the
+    // reference's initialize() normalises the still-zero psi); the fused paths
+    // and load_psi report them.
+    double calc_norm(bool to_host) override {
         materialize();
         enqueue_norm(cur, psi.p, /*set_divisor=*/false);
         set_divisor_one();
+        if (!to_host)
+            return 0.0;
         double x = 0;
         GPE_CUDA(cudaMemcpyAsync(&x, norm_state.p, sizeof(double), cudaMemcpyDeviceToHost, cur));
+        GPE_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int), cur));
         GPE_CUDA(cudaStreamSynchronize(cur));
-        check_status();
         return x;
     }
 
@@ -917,10 +934,17 @@ int gpe_imag_iter_nonlinear_step(gpe_handle *h) {
 int gpe_calc_norm(gpe_handle *h, double *x) {
     GPE_HANDLE(h);
     return guarded([&] {
-        double v = h->impl->calc_norm();
+        double v = h->impl->calc_norm(x != nullptr);
         if (x)
             *x = v;
     });
+}
+
+int gpe_import_psi(gpe_handle *h, const double *psi, size_t n) {
+    GPE_HANDLE(h);
+    if (!psi || n != h->impl->n())
+        return bad("gpe_import_psi: null pointer or n != nx*ny*nz");
+    return guarded([&] { h->impl->import_psi(psi); });
 }
 
 int gpe_normalize(gpe_handle *h) {

@@ -96,6 +96,11 @@ class B200GrossPitaevskiSolver:
         a = _as_c128_flat(psi, self.n)
         capi.check(self._L.gpe_load_psi(self._h, capi.dptr(a), self.n))
 
+    def import_data(self, psi) -> None:
+        """import_data: psi and psii take the values as given (no normalisation)."""
+        a = _as_c128_flat(psi, self.n)
+        capi.check(self._L.gpe_import_psi(self._h, capi.dptr(a), self.n))
+
     def load_pote(self, V) -> None:
         a = np.ascontiguousarray(np.asarray(V, dtype=np.float64).reshape(-1))
         if a.size != self.n:
@@ -123,7 +128,11 @@ class B200GrossPitaevskiSolver:
     def imag_iter_nonlinear_step(self) -> None:
         capi.check(self._L.gpe_imag_iter_nonlinear_step(self._h))
 
-    def calc_norm(self) -> float:
+    def calc_norm(self, to_host: bool = True) -> float:
+        """xnorma; with to_host=False the reduction stays on the device."""
+        if not to_host:
+            capi.check(self._L.gpe_calc_norm(self._h, None))
+            return self.xnorma
         x = ctypes.c_double()
         capi.check(self._L.gpe_calc_norm(self._h, ctypes.byref(x)))
         self.xnorma = x.value
@@ -154,7 +163,7 @@ class B200GrossPitaevskiSolver:
         self.calc_fi3d()
         self.imag_iter_linear_step()
         self.imag_iter_nonlinear_step()
-        self.calc_norm()
+        self.calc_norm(to_host=False)
         self.normalize()
 
     def real_time_iter(self) -> None:

@@ -99,6 +99,10 @@ int gpe_synchronize(gpe_handle *h);
  * scratch copy psii both take the given values, then calc_norm + normalize.
  * n = nx*ny*nz complex values (2n doubles). */
 int gpe_load_psi(gpe_handle *h, const double *psi_c128, size_t n);
+/* import_data (solver.hpp:69; gpu_solver.cpp:141-148): psi and psii take the given
+ * values as they are (no normalisation).  An adapter whose base class runs
+ * load_buffer itself calls this, then calc_norm and normalize. */
+int gpe_import_psi(gpe_handle *h, const double *psi_c128, size_t n);
 /* load_pote (solver.cpp:127-131). n = nx*ny*nz doubles. */
 int gpe_load_potential(gpe_handle *h, const double *V, size_t n);
 /* export_data: the current psi (normalised if the last step was an imaginary-time
@@ -112,7 +116,9 @@ int gpe_export_fi3d(gpe_handle *h, double *fi3d, size_t n);
 int gpe_calc_fi3d(gpe_handle *h);                 /* calc_fi3d (Poisson::execute) */
 int gpe_imag_iter_linear_step(gpe_handle *h);     /* fused Euler update into psii */
 int gpe_imag_iter_nonlinear_step(gpe_handle *h);  /* psi <- psii (nonlinear term is fused above) */
-int gpe_calc_norm(gpe_handle *h, double *xnorma); /* xnorma = sum |psi|^2 dV (FP64) */
+/* xnorma = sum |psi|^2 dV in FP64.  With xnorma == NULL the reduction stays on the
+ * device (no host synchronisation); normalize uses the device value either way. */
+int gpe_calc_norm(gpe_handle *h, double *xnorma);
 int gpe_normalize(gpe_handle *h);                 /* psi /= sqrt(xnorma) */
 int gpe_real_fft_potential_half_step(gpe_handle *h);
 int gpe_real_fft_kinetic_step(gpe_handle *h);
