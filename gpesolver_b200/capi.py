@@ -84,7 +84,12 @@ SIGNATURES = [
     ("gpe_launch_count", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     ("gpe_time_kernel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]),
     ("gpe_kernel_name", ctypes.c_char_p, [ctypes.c_int]),
+    ("gpe_calc_fi3d_noalloc", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),
 ]
+
+GPE_NOALLOC_SCRATCH_BYTES = 16 << 20
 
 KERNELS = ["DIP_Z_FWD", "DIP_Y_FWD", "DIP_X", "DIP_Y_INV", "DIP_Z_INV", "KIN_Z_FWD", "KIN_Y_FWD",
            "KIN_X", "KIN_Y_INV", "KIN_Z_INV", "PHASE", "IT_UPDATE"]

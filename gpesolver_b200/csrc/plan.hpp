@@ -10,6 +10,9 @@
 
 namespace gpe {
 
+// Message of the last failed gpe_* call on the calling thread (gpe_last_error).
+std::string &last_error();
+
 struct Error : std::runtime_error {
     int code;
     Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}

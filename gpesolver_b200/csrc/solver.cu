@@ -75,7 +75,10 @@ __global__ void k_set_f64(double *p, double v) { p[0] = v; }
 // ---------------------------------------------------------------------------
 // Error helpers
 // ---------------------------------------------------------------------------
-static thread_local std::string t_last_error;
+std::string &last_error() {
+    static thread_local std::string msg;
+    return msg;
+}
 
 #define GPE_CUDA(call)                                                                             \
     do {                                                                                           \
@@ -787,16 +790,16 @@ template <class F> int guarded(F &&f) {
         f();
         return GPE_OK;
     } catch (const gpe::Error &e) {
-        gpe::t_last_error = e.what();
+        gpe::last_error() = e.what();
         return e.code;
     } catch (const std::exception &e) {
-        gpe::t_last_error = e.what();
+        gpe::last_error() = e.what();
         return GPE_ERR_CUDA;
     }
 }
 
 int bad(const char *msg) {
-    gpe::t_last_error = msg;
+    gpe::last_error() = msg;
     return GPE_ERR_ARG;
 }
 
@@ -810,7 +813,7 @@ int bad(const char *msg) {
 
 extern "C" {
 
-const char *gpe_last_error(void) { return gpe::t_last_error.c_str(); }
+const char *gpe_last_error(void) { return gpe::last_error().c_str(); }
 int gpe_abi_version(void) { return GPE_B200_ABI_VERSION; }
 
 int gpe_params_derive(gpe_params *p) {

@@ -156,6 +156,31 @@ int gpe_time_kernel(gpe_handle *h, int which, int reps, double *ms_per_launch,
 /* Name of kernel `which` as it appears in a profiler's launch list. */
 const char *gpe_kernel_name(int which);
 
+/* --- allocation-free variant --- */
+
+/* Size of the file-scope device array gpe_calc_fi3d_noalloc works in. */
+#define GPE_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* calc_fi3d for callers that cannot allocate device memory (a framework that
+ * owns all device memory through its own allocator, or a loop that must not
+ * add the device-wide synchronisation cudaMalloc/cudaFree can cause).  This
+ * entry point has no counterpart in the reference.  It computes the dipolar
+ * field phi of a complex64 psi already on the device, with the same kernels as
+ * gpe_calc_fi3d, and allocates nothing: its intermediates live in one
+ * file-scope __device__ array of GPE_NOALLOC_SCRATCH_BYTES (16 MiB) that every
+ * GPU loading the library keeps until the process exits.
+ *   psi_c64_dev  device pointer, nx*ny*nz interleaved (re, im) floats, normalised psi
+ *   fi3d_dev     device pointer, nx*ny*nz floats (output)
+ *   n_atoms      w in rho = w |psi|^2
+ *   cuda_stream  cudaStream_t to launch on (NULL: the legacy default stream)
+ * Grids whose scratch exceeds the limit are rejected with GPE_ERR_SIZE
+ * (128 x 128 x 32 needs about 10.9 MB).  All calls on a GPU share the array, so
+ * calls that overlap on one GPU race.  The first call on each device does a
+ * one-time host-side set-up (device address of the array, kernel attributes);
+ * make it before any stream capture on that device. */
+int gpe_calc_fi3d_noalloc(const void *psi_c64_dev, float *fi3d_dev, int nx, int ny, int nz,
+                          double dx, double dy, double dz, double n_atoms, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
