@@ -408,6 +408,21 @@ def run_our_arm(args):
         dist.destroy_process_group()
 
 
+def run_profile(iters: int) -> None:
+    """A short run of the RT kernels for a profiler's launch list (no timing)."""
+    import gpesolver_b200 as G
+
+    p = G.params_from_json(workload_json())
+    with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
+        s.load_pote(G.potential(p))
+        s.load_buffer(G.initial_psi(p))
+        s.imag_steps(10)
+        s.load_pote(G.potential(p, "MEXICAN_FREE"))
+        s.real_steps(iters, 0)
+        s.synchronize()
+        print(f"profile run: {iters} RT iterations, {s.launch_count()} kernel launches", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -417,7 +432,13 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", type=int, default=0,
+                    help="profiling run: set up the workload (10 IT iterations), then run this many "
+                         "RT iterations untimed and exit")
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args.profile)
+        return
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

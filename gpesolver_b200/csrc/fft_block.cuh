@@ -11,8 +11,9 @@
 //
 // ping-ponging between two shared-memory buffers, so the output is in natural
 // order without a bit-reversal pass.  Twiddles come from a per-length table
-// exp(-2 pi i m / L), m < L, computed on the host in FP64 and rounded once to the
-// working precision; the inverse transform uses its conjugate.
+// exp(-2 pi i m / L), m < L, computed in FP64 and rounded once to the working
+// precision (in FP32 with a second table holding the rounding remainder, for a
+// compensated multiply); the inverse transform uses the conjugate.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -41,6 +42,30 @@ template <int SIGN, class C> __device__ __forceinline__ C mul_si(C a) {
 // a * W where W = cos + SIGN*i*sin
 template <int SIGN, class C, class R> __device__ __forceinline__ C mul_w(C a, R c, R s) {
     return SIGN > 0 ? C{a.x * c - a.y * s, a.x * s + a.y * c} : C{a.x * c + a.y * s, a.y * c - a.x * s};
+}
+
+// Twiddles are applied with a compensated multiply in FP32: each twiddle is
+// split as hi + lo (hi = the float nearest the exact value, lo = the float
+// nearest the remainder) and x*c is evaluated as fma(x, hi, x*lo), which rounds
+// once to the correctly rounded x*c.  A plain FP32 twiddle carries a fixed
+// modulus error (2 fl32(sqrt(1/2))^2 - 1 = -3.4e-8, c8^2 + s8^2 - 1 = -5.7e-8,
+// and a net negative mean over a twiddle table) that every butterfly applies
+// with the same sign, so the norm of psi drifted by ~5e-8 per FFT round trip;
+// compensated, the drift is at the 1e-11 noise level.
+template <class R> __device__ __forceinline__ R cmulk(R x, double c) {
+    if constexpr (sizeof(R) == 4) {
+        const float hi = (float)c;
+        const float lo = (float)(c - (double)hi);
+        return fmaf(x, hi, x * lo);
+    } else {
+        return x * c;
+    }
+}
+// a * W where W = c + SIGN*i*s, compensated
+template <int SIGN, class C, class R> __device__ __forceinline__ C mul_wk(C a, double c, double s) {
+    if (SIGN > 0)
+        return C{cmulk<R>(a.x, c) - cmulk<R>(a.y, s), cmulk<R>(a.x, s) + cmulk<R>(a.y, c)};
+    return C{cmulk<R>(a.x, c) + cmulk<R>(a.y, s), cmulk<R>(a.y, c) - cmulk<R>(a.x, s)};
 }
 
 // cos / sin of 2 pi m / 16 (the twiddles of the radix-8 and radix-16 kernels)
@@ -107,8 +132,12 @@ template <int N1, int N2, int SIGN, class R> struct DFTSplit {
 #pragma unroll
             for (int k1 = 0; k1 < N1; ++k1) {
                 const int m = (n2 * k1 * (16 / N)) & 15;
-                if (m != 0)
-                    y[n2][k1] = mul_w<SIGN>(y[n2][k1], (R)cos16(m), (R)sin16(m));
+                if (m == 4 || m == 12)
+                    y[n2][k1] = (m == 4) == (SIGN > 0) ? mul_si<+1>(y[n2][k1]) : mul_si<-1>(y[n2][k1]);
+                else if (m == 8)
+                    y[n2][k1] = C{-y[n2][k1].x, -y[n2][k1].y};
+                else if (m != 0)
+                    y[n2][k1] = mul_wk<SIGN, C, R>(y[n2][k1], cos16(m), sin16(m));
             }
         }
 #pragma unroll
@@ -192,7 +221,7 @@ template <int P, int SIGN, class R> struct DFTOdd {
 #pragma unroll
             for (int k = 1; k < P; ++k) {
                 const int m = (k * q) % P;
-                acc         = cadd(acc, mul_w<SIGN>(a[k], (R)OddTab<P>::c(m), (R)OddTab<P>::s(m)));
+                acc         = cadd(acc, mul_wk<SIGN, C, R>(a[k], OddTab<P>::c(m), OddTab<P>::s(m)));
             }
             out[q] = acc;
         }
@@ -216,20 +245,32 @@ struct LinePlan {
     int L;
     int nstages;
     int radix[8];
-    const void *tw; // cplx<R>[L]: exp(-2 pi i m / L)
+    const void *tw;   // cplx<R>[L]: exp(-2 pi i m / L), rounded to R
+    const void *twlo; // FP32 only: cplx<R>[L], the rounding remainder of tw
 };
+
+// v * w (SIGN < 0) or v * conj(w) (SIGN > 0) with w = hi + lo (compensated).
+template <int SIGN, class C> __device__ __forceinline__ C twmul(C v, C hi, C lo) {
+    const float sh = SIGN < 0 ? hi.y : -hi.y, sl = SIGN < 0 ? lo.y : -lo.y;
+    const float cre = v.x * lo.x - v.y * sl;
+    const float cim = v.x * sl + v.y * lo.x;
+    return C{fmaf(v.x, hi.x, fmaf(-v.y, sh, cre)), fmaf(v.x, sh, fmaf(v.y, hi.x, cim))};
+}
 
 template <int RADIX, int SIGN, class R>
 __device__ __forceinline__ void fft_stage(const cplx<R> *__restrict__ src, cplx<R> *__restrict__ dst,
                                           int L, int Ns, int count, int bs, int ts,
-                                          const cplx<R> *__restrict__ tw, int tid, int nthreads) {
+                                          const cplx<R> *__restrict__ tw,
+                                          const cplx<R> *__restrict__ twlo, int tid, int nthreads) {
     using C         = cplx<R>;
     const int nr    = L / RADIX;
     const int step  = L / (Ns * RADIX);
     const int items = count * nr;
+    // consecutive threads take consecutive lines b: with the tile layouts used
+    // here (bs = 1) their shared-memory accesses fall in distinct banks.
     for (int it = tid; it < items; it += nthreads) {
-        const int b  = it / nr;
-        const int j  = it - b * nr;
+        const int j  = it / count;
+        const int b  = it - j * count;
         const int jm = j % Ns;
         C a[RADIX];
         const C *s = src + (size_t)b * bs + (size_t)j * ts;
@@ -237,8 +278,12 @@ __device__ __forceinline__ void fft_stage(const cplx<R> *__restrict__ src, cplx<
         for (int k = 0; k < RADIX; ++k) {
             C v = s[(size_t)k * nr * ts];
             if (k > 0 && jm > 0) {
-                const C w = __ldg(&tw[jm * k * step]); // < Ns * RADIX * step = L
-                v         = SIGN < 0 ? cmul(v, w) : cmulc(v, w);
+                const int t = jm * k * step; // < Ns * RADIX * step = L
+                const C w   = __ldg(&tw[t]);
+                if constexpr (sizeof(R) == 4)
+                    v = twmul<SIGN>(v, w, __ldg(&twlo[t]));
+                else
+                    v = SIGN < 0 ? cmul(v, w) : cmulc(v, w);
             }
             a[k] = v;
         }
@@ -262,16 +307,17 @@ __device__ cplx<R> *block_fft(cplx<R> *buf0, cplx<R> *buf1, const LinePlan &ln, 
     C *dst      = buf1;
     int Ns      = 1;
     const C *tw = reinterpret_cast<const C *>(ln.tw);
+    const C *tl = reinterpret_cast<const C *>(ln.twlo);
     for (int s = 0; s < ln.nstages; ++s) {
         const int r = ln.radix[s];
         switch (r) {
-        case 2: fft_stage<2, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tid, nthreads); break;
-        case 3: fft_stage<3, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tid, nthreads); break;
-        case 4: fft_stage<4, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tid, nthreads); break;
-        case 5: fft_stage<5, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tid, nthreads); break;
-        case 7: fft_stage<7, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tid, nthreads); break;
-        case 8: fft_stage<8, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tid, nthreads); break;
-        default: fft_stage<16, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tid, nthreads); break;
+        case 2: fft_stage<2, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tl, tid, nthreads); break;
+        case 3: fft_stage<3, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tl, tid, nthreads); break;
+        case 4: fft_stage<4, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tl, tid, nthreads); break;
+        case 5: fft_stage<5, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tl, tid, nthreads); break;
+        case 7: fft_stage<7, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tl, tid, nthreads); break;
+        case 8: fft_stage<8, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tl, tid, nthreads); break;
+        default: fft_stage<16, SIGN, R>(src, dst, ln.L, Ns, count, bs, ts, tw, tl, tid, nthreads); break;
         }
         __syncthreads();
         C *t = src;

@@ -49,8 +49,9 @@ __global__ void __launch_bounds__(256)
     k_dip_z_fwd(const cplx<R> *__restrict__ psi, const double *__restrict__ norm_state, int lazy,
                 cplx<R> *__restrict__ A, int nx, int ny, int nz, R w, LinePlan ln, int TB) {
     using C         = cplx<R>;
+    const int TS    = TB + 1; // odd tile stride: the transposing loads hit distinct banks
     C *b0           = reinterpret_cast<C *>(g_smem);
-    C *b1           = b0 + (size_t)TB * ln.L;
+    C *b1           = b0 + (size_t)TS * ln.L;
     const int H     = nz + 1;
     const int lines = nx * ny;
     const int l0    = blockIdx.x * TB;
@@ -59,18 +60,18 @@ __global__ void __launch_bounds__(256)
     for (int e = threadIdx.x; e < cnt * nz; e += blockDim.x) {
         const int b = e / nz, k = e - b * nz;
         const C v   = psi[(size_t)(l0 + b) * nz + k];
-        b0[k * TB + b] = C{(v.x * v.x + v.y * v.y) * ws, (R)0};
+        b0[k * TS + b] = C{(v.x * v.x + v.y * v.y) * ws, (R)0};
     }
     for (int e = threadIdx.x; e < cnt * (ln.L - nz); e += blockDim.x) {
         const int b = e % cnt, k = nz + e / cnt;
-        b0[k * TB + b] = C{(R)0, (R)0};
+        b0[k * TS + b] = C{(R)0, (R)0};
     }
     __syncthreads();
-    C *res = block_fft<-1, R>(b0, b1, ln, cnt, 1, TB, threadIdx.x, blockDim.x);
+    C *res = block_fft<-1, R>(b0, b1, ln, cnt, 1, TS, threadIdx.x, blockDim.x);
     for (int e = threadIdx.x; e < cnt * H; e += blockDim.x) {
         const int b = e / H, kz = e - b * H;
         const int l = l0 + b, i = l / ny, j = l - i * ny;
-        A[((size_t)i * 2 * ny + j) * H + kz] = res[kz * TB + b];
+        A[((size_t)i * 2 * ny + j) * H + kz] = res[kz * TS + b];
     }
 }
 
@@ -152,8 +153,9 @@ __global__ void __launch_bounds__(256)
     k_dip_z_inv(const cplx<R> *__restrict__ A, R *__restrict__ phi, int nx, int ny, int nz, R inv_n,
                 LinePlan ln, int TB) {
     using C         = cplx<R>;
+    const int TS    = TB + 1;
     C *b0           = reinterpret_cast<C *>(g_smem);
-    C *b1           = b0 + (size_t)TB * ln.L;
+    C *b1           = b0 + (size_t)TS * ln.L;
     const int H     = nz + 1;
     const int L     = ln.L; // 2nz
     const int lines = nx * ny;
@@ -170,13 +172,13 @@ __global__ void __launch_bounds__(256)
             const C u = line[L - m];
             v         = C{u.x, -u.y};
         }
-        b0[m * TB + b] = v;
+        b0[m * TS + b] = v;
     }
     __syncthreads();
-    C *res = block_fft<+1, R>(b0, b1, ln, cnt, 1, TB, threadIdx.x, blockDim.x);
+    C *res = block_fft<+1, R>(b0, b1, ln, cnt, 1, TS, threadIdx.x, blockDim.x);
     for (int e = threadIdx.x; e < cnt * nz; e += blockDim.x) {
         const int b = e / nz, k = e - b * nz;
-        phi[(size_t)(l0 + b) * nz + k] = res[k * TB + b].x * inv_n;
+        phi[(size_t)(l0 + b) * nz + k] = res[k * TS + b].x * inv_n;
     }
 }
 
@@ -190,20 +192,21 @@ template <int SIGN, class R>
 __global__ void __launch_bounds__(256)
     k_kin_z(cplx<R> *__restrict__ psi, int lines, int nz, LinePlan ln, int TB) {
     using C       = cplx<R>;
+    const int TS  = TB + 1;
     C *b0         = reinterpret_cast<C *>(g_smem);
-    C *b1         = b0 + (size_t)TB * ln.L;
+    C *b1         = b0 + (size_t)TS * ln.L;
     const int l0  = blockIdx.x * TB;
     const int cnt = min(TB, lines - l0);
     C *base       = psi + (size_t)l0 * nz;
     for (int e = threadIdx.x; e < cnt * nz; e += blockDim.x) {
         const int b = e / nz, k = e - b * nz;
-        b0[k * TB + b] = base[e];
+        b0[k * TS + b] = base[e];
     }
     __syncthreads();
-    C *res = block_fft<SIGN, R>(b0, b1, ln, cnt, 1, TB, threadIdx.x, blockDim.x);
+    C *res = block_fft<SIGN, R>(b0, b1, ln, cnt, 1, TS, threadIdx.x, blockDim.x);
     for (int e = threadIdx.x; e < cnt * nz; e += blockDim.x) {
         const int b = e / nz, k = e - b * nz;
-        base[e]     = res[k * TB + b];
+        base[e]     = res[k * TS + b];
     }
 }
 
@@ -230,12 +233,26 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Unit-modulus factor applied as v + v*w with w = exp(i theta) - 1 given to
+// full relative precision: the factor's modulus error is then ~eps*theta^2
+// instead of ~eps, so repeated application does not bias the norm.
+template <class C> __device__ __forceinline__ C apply_wm1(C v, C w) {
+    return C{v.x + (v.x * w.x - v.y * w.y), v.y + (v.x * w.y + v.y * w.x)};
+}
+// (1+a)(1+b)(1+c) - 1 for small a, b, c
+template <class C> __device__ __forceinline__ C combine_wm1(C a, C b, C c) {
+    const C ab = cadd(cadd(a, b), cmul(a, b));
+    return cadd(cadd(ab, c), cmul(ab, c));
+}
+
 // x lines for TB consecutive (j, k) columns: forward FFT, multiply by the
-// separable kinetic phase ex[i] * ey[j] * ez[k] (1/N folded into ex), inverse.
+// kinetic phase exp(i(-dt/2m)(kx^2 + ky^2 + kz^2)) built from per-axis tables of
+// exp(i theta) - 1 (FP64-computed), scale by 1/N = inv_hi + inv_lo, inverse.
 template <class R>
 __global__ void __launch_bounds__(256)
     k_kin_x(cplx<R> *__restrict__ psi, const cplx<R> *__restrict__ ex, const cplx<R> *__restrict__ ey,
-            const cplx<R> *__restrict__ ez, int nx, int ny, int nz, LinePlan ln, int TB) {
+            const cplx<R> *__restrict__ ez, R inv_hi, R inv_lo, int nx, int ny, int nz, LinePlan ln,
+            int TB) {
     using C         = cplx<R>;
     C *b0           = reinterpret_cast<C *>(g_smem);
     C *b1           = b0 + (size_t)TB * ln.L;
@@ -252,8 +269,9 @@ __global__ void __launch_bounds__(256)
     for (int e = threadIdx.x; e < cnt * nx; e += blockDim.x) {
         const int i = e / cnt, b = e - i * cnt;
         const int c = c0 + b, j = c / nz, k = c - j * nz;
-        const C ph  = cmul(cmul(__ldg(&ex[i]), __ldg(&ey[j])), __ldg(&ez[k]));
-        res[i * TB + b] = cmul(res[i * TB + b], ph);
+        const C w   = combine_wm1(__ldg(&ex[i]), __ldg(&ey[j]), __ldg(&ez[k]));
+        const C v   = apply_wm1(res[i * TB + b], w);
+        res[i * TB + b] = C{fma(v.x, inv_lo, v.x * inv_hi), fma(v.y, inv_lo, v.y * inv_hi)};
     }
     __syncthreads();
     C *res2 = block_fft<+1, R>(res, other, ln, cnt, 1, TB, threadIdx.x, blockDim.x);
@@ -289,9 +307,11 @@ __global__ void __launch_bounds__(256)
         const R a       = sqrt(dens);
         const R v_int   = g3w * dens + gw15 * (a * a * a);
         const R total   = V[q] + cdd * phi[q] + v_int;
+        // exp(i theta) - 1 = (-2 sin^2(theta/2), sin(theta)), theta = -dt/2 * total
         R s, c;
-        sincos_r<R>(-half_dt * total, &s, &c);
-        psi[q] = C{p.x * c - p.y * s, p.x * s + p.y * c};
+        sincos_r<R>((R)-0.5 * half_dt * total, &s, &c);
+        const C w = C{(R)-2 * s * s, (R)2 * s * c};
+        psi[q]    = apply_wm1(p, w);
     }
 }
 

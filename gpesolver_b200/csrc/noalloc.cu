@@ -12,7 +12,7 @@
 // Limits and sharing:
 //  * scratch holds the pruned dipolar spectrum (nx * 2ny * (nz+1) complex64),
 //    the V_dd(k) table ((nx+1) * (ny+1) * (nz+1) floats) and three twiddle
-//    tables; grids needing more than GPE_NOALLOC_SCRATCH_BYTES are rejected
+//    tables with their rounding remainders; grids needing more than GPE_NOALLOC_SCRATCH_BYTES are rejected
 //    with GPE_ERR_SIZE (128 x 128 x 32 needs about 10.9 MB);
 //  * the array lives on every GPU that loads the library until the process
 //    exits, and every call on a GPU shares it: calls that overlap on that GPU
@@ -52,12 +52,15 @@ NoallocSlot g_noalloc_slots[kMaxDevices];
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
-// exp(-2 pi i m / L) in FP64, rounded to float2.
-__global__ void k_na_twiddles(float2 *tw, int L) {
+// exp(-2 pi i m / L) in FP64, rounded to float2 (tw) with the rounding
+// remainder in twlo (the FFT stages multiply by tw + twlo, compensated).
+__global__ void k_na_twiddles(float2 *tw, float2 *twlo, int L) {
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < L; m += gridDim.x * blockDim.x) {
         double s, c;
         sincospi(2.0 * (double)m / (double)L, &s, &c);
-        tw[m] = make_float2((float)c, (float)-s);
+        const float ch = (float)c, sh = (float)-s;
+        tw[m]          = make_float2(ch, sh);
+        twlo[m]        = make_float2((float)(c - (double)ch), (float)(-s - (double)sh));
     }
 }
 
@@ -78,6 +81,7 @@ __global__ void k_na_vdip(float *vk, int nx, int ny, int nz, double dx, double d
 
 struct Layout {
     size_t a_off, vk_off, twx_off, twy_off, twz_off, total;
+    // each twiddle region holds the table followed by its remainder table
 };
 
 Layout layout(int nx, int ny, int nz) {
@@ -89,18 +93,18 @@ Layout layout(int nx, int ny, int nz) {
     l.vk_off = off;
     off += align256(sizeof(float) * (size_t)(nx + 1) * (ny + 1) * H);
     l.twx_off = off;
-    off += align256(sizeof(float2) * 2 * (size_t)nx);
+    off += align256(sizeof(float2) * 2 * 2 * (size_t)nx);
     l.twy_off = off;
-    off += align256(sizeof(float2) * 2 * (size_t)ny);
+    off += align256(sizeof(float2) * 2 * 2 * (size_t)ny);
     l.twz_off = off;
-    off += align256(sizeof(float2) * 2 * (size_t)nz);
+    off += align256(sizeof(float2) * 2 * 2 * (size_t)nz);
     l.total = off;
     return l;
 }
 
-int tile_for(int L) {
+int tile_for(int L, int pad) {
     int TB = 32;
-    while (TB > 1 && 2 * sizeof(float2) * (size_t)TB * L > 64 * 1024)
+    while (TB > 1 && 2 * sizeof(float2) * (size_t)(TB + pad) * L > 64 * 1024)
         TB >>= 1;
     return TB;
 }
@@ -154,10 +158,10 @@ extern "C" int gpe_calc_fi3d_noalloc(const void *psi_c64_dev, float *fi3d_dev, i
     if (dev < 0 || dev >= kMaxDevices)
         return fail(GPE_ERR_ARG, "gpe_calc_fi3d_noalloc: device ordinal out of range");
     cudaStream_t s = (cudaStream_t)cuda_stream;
-    const int TBx = tile_for(lx.L), TBy = tile_for(ly.L), TBz = tile_for(lz.L);
+    const int TBx = tile_for(lx.L, 0), TBy = tile_for(ly.L, 0), TBz = tile_for(lz.L, 1);
     const size_t smx = 2 * sizeof(float2) * (size_t)TBx * lx.L;
     const size_t smy = 2 * sizeof(float2) * (size_t)TBy * ly.L;
-    const size_t smz = 2 * sizeof(float2) * (size_t)TBz * lz.L;
+    const size_t smz = 2 * sizeof(float2) * (size_t)(TBz + 1) * lz.L; // z tiles: odd stride TB + 1
 
     NoallocSlot &slot = g_noalloc_slots[dev];
     bool rebuild      = false;
@@ -201,12 +205,15 @@ extern "C" int gpe_calc_fi3d_noalloc(const void *psi_c64_dev, float *fi3d_dev, i
     lx.tw               = twx;
     ly.tw               = twy;
     lz.tw               = twz;
+    lx.twlo             = twx + 2 * nx;
+    ly.twlo             = twy + 2 * ny;
+    lz.twlo             = twz + 2 * nz;
     const int H         = nz + 1;
 
     if (rebuild) {
-        k_na_twiddles<<<(2 * nx + 255) / 256, 256, 0, s>>>(twx, 2 * nx);
-        k_na_twiddles<<<(2 * ny + 255) / 256, 256, 0, s>>>(twy, 2 * ny);
-        k_na_twiddles<<<(2 * nz + 255) / 256, 256, 0, s>>>(twz, 2 * nz);
+        k_na_twiddles<<<(2 * nx + 255) / 256, 256, 0, s>>>(twx, twx + 2 * nx, 2 * nx);
+        k_na_twiddles<<<(2 * ny + 255) / 256, 256, 0, s>>>(twy, twy + 2 * ny, 2 * ny);
+        k_na_twiddles<<<(2 * nz + 255) / 256, 256, 0, s>>>(twz, twz + 2 * nz, 2 * nz);
         k_na_vdip<<<592, 256, 0, s>>>(vk, nx, ny, nz, dx, dy, dz);
     }
     // The pruned dipolar convolution: every element of A that a pass reads was

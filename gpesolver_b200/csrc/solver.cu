@@ -147,9 +147,10 @@ template <class R> class Solver final : public SolverBase {
     // A planned line transform plus its launch tile.
     struct Line {
         LinePlan plan{};
-        DevBuf<C> tw;
-        int TB = 1;
-        size_t smem() const { return 2 * sizeof(C) * (size_t)TB * plan.L; }
+        DevBuf<C> tw, twlo;
+        int TB  = 1;
+        int pad = 0; // z-pass tiles use the odd stride TB + 1
+        size_t smem() const { return 2 * sizeof(C) * (size_t)(TB + pad) * plan.L; }
     };
 
   public:
@@ -170,12 +171,12 @@ template <class R> class Solver final : public SolverBase {
         GPE_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
         cur = own_stream;
 
-        plan_line(kz, nz, 16);
-        plan_line(ky, ny, 32);
-        plan_line(kx, nx, 32);
-        plan_line(dz, 2 * nz, 16);
-        plan_line(dy, 2 * ny, 32);
-        plan_line(dx, 2 * nx, 32);
+        plan_line(kz, nz, 16, 1);
+        plan_line(ky, ny, 32, 0);
+        plan_line(kx, nx, 32, 0);
+        plan_line(dz, 2 * nz, 16, 1);
+        plan_line(dy, 2 * ny, 32, 0);
+        plan_line(dx, 2 * nx, 32, 0);
 
         psi.alloc(N);
         psii.alloc(N);
@@ -455,7 +456,7 @@ template <class R> class Solver final : public SolverBase {
                 break;
             case GPE_K_KIN_X:
                 launch(k_kin_x<R>, (ny * nz + kx.TB - 1) / kx.TB, 256, kx.smem(), cur, psi.p,
-                       (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, nx, ny, nz, kx.plan, kx.TB);
+                       (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, nx, ny, nz, kx.plan, kx.TB);
                 b = 2 * F;
                 break;
             case GPE_K_PHASE:
@@ -507,6 +508,7 @@ template <class R> class Solver final : public SolverBase {
     std::map<std::tuple<int, int, const void *>, cudaGraphExec_t> graphs;
     std::map<std::tuple<int, int, const void *>, int> graph_nodes;
     int nblk_elem = 0;
+    R inv_hi = 0, inv_lo = 0;
     bool lazy     = false;
     double ggp11_cur = 0, gamma_cur = 0;
     long long n_launch = 0;
@@ -523,25 +525,31 @@ template <class R> class Solver final : public SolverBase {
         ++n_launch;
     }
 
-    void plan_line(Line &ln, int L, int tbmax) {
+    void plan_line(Line &ln, int L, int tbmax, int pad) {
         std::vector<int> r = factor_line(L);
         ln.plan.L          = L;
         ln.plan.nstages    = (int)r.size();
+        ln.pad             = pad;
         for (size_t s = 0; s < r.size(); ++s)
             ln.plan.radix[s] = r[s];
         std::vector<double> t = twiddles(L);
-        std::vector<C> tc(L);
-        for (int m = 0; m < L; ++m)
+        std::vector<C> tc(L), tl(L);
+        for (int m = 0; m < L; ++m) {
             tc[m] = C{(R)t[2 * m], (R)t[2 * m + 1]};
+            tl[m] = C{(R)(t[2 * m] - (double)tc[m].x), (R)(t[2 * m + 1] - (double)tc[m].y)};
+        }
         ln.tw.alloc(L);
+        ln.twlo.alloc(L);
         GPE_CUDA(cudaMemcpy(ln.tw.p, tc.data(), sizeof(C) * L, cudaMemcpyHostToDevice));
-        ln.plan.tw = ln.tw.p;
+        GPE_CUDA(cudaMemcpy(ln.twlo.p, tl.data(), sizeof(C) * L, cudaMemcpyHostToDevice));
+        ln.plan.tw   = ln.tw.p;
+        ln.plan.twlo = ln.twlo.p;
         // Tile: two Stockham buffers of TB lines within a 64 KiB budget per CTA.
         const size_t budget = 64 * 1024;
         int TB              = tbmax;
-        while (TB > 1 && 2 * sizeof(C) * (size_t)TB * L > budget)
+        while (TB > 1 && 2 * sizeof(C) * (size_t)(TB + pad) * L > budget)
             TB >>= 1;
-        if (2 * sizeof(C) * (size_t)TB * L > 200 * 1024)
+        if (2 * sizeof(C) * (size_t)(TB + pad) * L > 200 * 1024)
             throw Error(GPE_ERR_SIZE, "FFT line of length " + std::to_string(L) + " too long");
         ln.TB = TB;
     }
@@ -588,21 +596,28 @@ template <class R> class Solver final : public SolverBase {
             GPE_CUDA(cudaMemcpy(vk.p, t.data(), sizeof(R) * t.size(), cudaMemcpyHostToDevice));
         }
         {
+            // Per-axis exp(i theta) - 1 with theta = -dt/(2m) k^2 (k as in
+            // fftw_split_solver.cpp:26-31), in FP64; the kernel combines the three
+            // axes and applies the factor as v + v*w.
             const double dt = P.real_time_dt, fac = -dt / (2.0 * P.m);
-            auto axis = [&](int n, double d, double scale, DevBuf<C> &out) {
+            auto axis = [&](int n, double d, DevBuf<C> &out) {
                 std::vector<C> t(n);
                 for (int i = 0; i < n; ++i) {
                     const double kv = (i <= n / 2) ? (2.0 * M_PI * i / (n * d))
                                                    : (2.0 * M_PI * (i - n) / (n * d));
                     const double f  = fac * (kv * kv);
-                    t[i]            = C{(R)(std::cos(f) * scale), (R)(std::sin(f) * scale)};
+                    const double sh = std::sin(0.5 * f);
+                    t[i]            = C{(R)(-2.0 * sh * sh), (R)std::sin(f)};
                 }
                 out.alloc(n);
                 GPE_CUDA(cudaMemcpy(out.p, t.data(), sizeof(C) * n, cudaMemcpyHostToDevice));
             };
-            axis(nx, P.dx, 1.0 / (double)N, ex);
-            axis(ny, P.dy, 1.0, ey);
-            axis(nz, P.dz, 1.0, ez);
+            axis(nx, P.dx, ex);
+            axis(ny, P.dy, ey);
+            axis(nz, P.dz, ez);
+            const double inv = 1.0 / (double)N;
+            inv_hi           = (R)inv;
+            inv_lo           = (R)(inv - (double)inv_hi);
         }
         one_buf.alloc(1);
         const double one = 1.0;
@@ -693,7 +708,7 @@ template <class R> class Solver final : public SolverBase {
                ky.plan, ky.TB);
         const int cols = ny * nz;
         launch(k_kin_x<R>, (cols + kx.TB - 1) / kx.TB, 256, kx.smem(), s, psi.p, (const C *)ex.p,
-               (const C *)ey.p, (const C *)ez.p, nx, ny, nz, kx.plan, kx.TB);
+               (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, nx, ny, nz, kx.plan, kx.TB);
         launch(k_kin_y<+1, R>, dim3((nz + ky.TB - 1) / ky.TB, nx), 256, ky.smem(), s, psi.p, ny, nz,
                ky.plan, ky.TB);
         launch(k_kin_z<+1, R>, (lines + kz.TB - 1) / kz.TB, 256, kz.smem(), s, psi.p, lines, nz,

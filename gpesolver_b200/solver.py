@@ -15,6 +15,7 @@ moves host buffers and sequences calls.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 from collections import namedtuple
 from typing import Callable, Optional
 
@@ -46,7 +47,9 @@ def make_gpe_params(p: PhysicalParameters, precision: str = "c64", device: int =
 
 class B200GrossPitaevskiSolver:
     def __init__(self, params: PhysicalParameters, precision: str = "c64", device: int = 0):
-        self.params = params
+        # the solver owns its parameters (real_steps advances edd on this copy,
+        # as calc_evolution advances the reference's singleton)
+        self.params = dataclasses.replace(params)
         self.precision = precision
         self._L = capi.lib()
         self._gp = make_gpe_params(params, precision, device)

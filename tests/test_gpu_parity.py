@@ -115,8 +115,36 @@ def test_virtual_by_virtual_iterations_match_fused(prec):
     assert rel_l2(outs[0], outs[1]) < (1e-13 if prec == "c128" else 1e-6)
 
 
-@pytest.mark.parametrize("k", [1, 2, 63, 64, 65, 130])
-def test_chunk_boundaries_imag_and_real(k):
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+@pytest.mark.parametrize("k", [63, 64, 65, 130])
+def test_fused_chunks_equal_single_iterations(k, prec):
+    # The fused paths replay CUDA graphs of 64 (IT) / 32 (RT) iterations plus a
+    # remainder graph; k calls of one iteration must give the same bits.
+    cfg = O.default_config(nx=32, ny=32, nz=16, init_strategy="GAUSS", pote_strategy="HARMONIC",
+                           edd=None, edd_start=1.3, edd_stop=1.6, iter_real=200)
+    p = gparams(cfg)
+    out = []
+    for fused in (True, False):
+        with G.B200GrossPitaevskiSolver(p, precision=prec) as s:
+            s.load_pote(G.potential(p))
+            s.load_buffer(G.initial_psi(p))
+            if fused:
+                s.imag_steps(k)
+                s.real_steps(k, 7)
+            else:
+                for t in range(k):
+                    s.imag_steps(1)
+                for t in range(k):
+                    s.real_steps(1, 7 + t)
+            out.append(s.export_data())
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("k", [1, 2, 33])
+def test_short_runs_match_oracle_with_edd_ramp(k):
+    # (this 32^2 x 16 box holds a collapsed droplet whose RT dynamics amplify
+    # rounding differences about tenfold every 20 iterations, so the FP64 parity
+    # bound applies to short runs)
     cfg = O.default_config(nx=32, ny=32, nz=16, init_strategy="GAUSS", pote_strategy="HARMONIC",
                            edd=None, edd_start=1.3, edd_stop=1.6, iter_real=200)
     p = gparams(cfg)
@@ -131,7 +159,7 @@ def test_chunk_boundaries_imag_and_real(k):
         got = s.export_data()
     want = c128(ref.psi())
     ref.close()
-    assert rel_l2(got, want) < 1e-10
+    assert rel_l2(got, want) < 1e-11
 
 
 def test_readme_config_imaginary_time_c64():
@@ -188,7 +216,9 @@ def test_real_time_conserves_norm_at_256():
         s.real_steps(200, 0)
         n1 = s.calc_norm()
     assert abs(n0 - 1.0) < 1e-6
-    assert abs(n1 - n0) < 1e-5
+    # FP32 norm drift over 200 iterations (unit-modulus factors applied as
+    # v + v(e^{i theta} - 1), compensated butterfly constants)
+    assert abs(n1 - n0) < 2e-6
 
 
 def test_nonfinite_state_is_reported():
