@@ -351,9 +351,8 @@ def run_our_arm(args):
     e2e_value = total_iters / (e2e_ms / 1e3)
 
     # ---- per-kernel roofline (kernels timed alone) ---------------------------
-    per_step_count = {"DIP_Z_FWD": 1, "DIP_Y_FWD": 1, "DIP_X": 1, "DIP_Y_INV": 1, "DIP_Z_INV": 1,
-                      "KIN_Z_FWD": 1, "KIN_Y_FWD": 1, "KIN_X": 1, "KIN_Y_INV": 1, "KIN_Z_INV": 1,
-                      "PHASE": 2}
+    # kernels of one RT iteration in the schedule the solver uses
+    per_step_count = {"F_X": 1, "F_YINV": 1, "F_Z": 1, "F_YFWD": 1}
     L = capi.lib()
     kt = {}
     import ctypes

@@ -47,8 +47,11 @@ class gpe_params(ctypes.Structure):
         ("const_edd", ctypes.c_int),
         ("edd", ctypes.c_double), ("edd_start", ctypes.c_double), ("edd_stop", ctypes.c_double),
         ("iter_real", ctypes.c_long),
-        ("precision", ctypes.c_int), ("device", ctypes.c_int),
+        ("precision", ctypes.c_int), ("device", ctypes.c_int), ("schedule", ctypes.c_int),
     ]
+
+GPE_SCHED_AUTO = 0
+GPE_SCHED_SPLIT = 1
 
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -92,7 +95,7 @@ SIGNATURES = [
 GPE_NOALLOC_SCRATCH_BYTES = 16 << 20
 
 KERNELS = ["DIP_Z_FWD", "DIP_Y_FWD", "DIP_X", "DIP_Y_INV", "DIP_Z_INV", "KIN_Z_FWD", "KIN_Y_FWD",
-           "KIN_X", "KIN_Y_INV", "KIN_Z_INV", "PHASE", "IT_UPDATE"]
+           "KIN_X", "KIN_Y_INV", "KIN_Z_INV", "PHASE", "IT_UPDATE", "F_X", "F_YINV", "F_Z", "F_YFWD"]
 
 
 def lib() -> ctypes.CDLL:

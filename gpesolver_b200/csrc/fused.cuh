@@ -1,0 +1,502 @@
+// Fused iteration pipeline (compile-time line lengths).
+//
+// One imaginary- or real-time iteration is four kernels, each a batch of 1D
+// FFT lines along one axis with the elementwise physics fused into its loads
+// and stores:
+//
+//   X  pencils along x: kinetic  fwd FFT(nx) * exp(i(-dt/2m)k^2)/N * inv FFT(nx)
+//                       dipolar  fwd FFT(2nx, upper half zero) * V_dd(k) * scale
+//                                * inv FFT(2nx), first nx kept
+//   Yi lines along y, inverse:   kinetic iFFT(ny); dipolar iFFT(2ny), first ny kept
+//   Z  rows along z:   dipolar C2R (pairs of rows packed in one complex FFT of
+//                      2nz) -> phi; kinetic iFFT(nz) -> psi; the real-time phases
+//                      of two consecutive half steps merged into one rotation
+//                      (they see the same |psi|, V and phi); rho = w|psi|^2;
+//                      kinetic FFT(nz); dipolar R2C (pairs) -> spectrum
+//                      (imaginary time: the Euler stencil update instead of the
+//                      kinetic transforms, with the norm reduced on the fly)
+//   Yf lines along y, forward:   kinetic FFT(ny); dipolar FFT(2ny, upper half zero)
+//
+// Dipolar spectrum layout: S[i][ky][kz-1], i < nx (x in real space between the
+// X passes), ky < 2ny, 1 <= kz <= nz.  The kz = 0 plane is not stored: V_dd is
+// kz^2/k^2, exactly 0 on that plane (fftw_poisson_solver.cpp:39-45), so it adds
+// nothing to phi.
+#pragma once
+
+#include "ct_fft.cuh"
+#include "kernels.cuh"
+
+namespace gpe {
+
+// Tile widths (lines per CTA) for a pass of line length L in precision R:
+// CNT*L complex within 32 KiB (one in-place tile buffer per CTA).
+template <class R, int L> constexpr int tile_lines() {
+    int c = (int)(32768 / (int)sizeof(cplx<R>) / L);
+    int p = 1;
+    while (p * 2 <= c && p * 2 <= 32)
+        p *= 2;
+    return p;
+}
+
+struct Twid {
+    const void *tw;
+    const void *lo;
+};
+
+struct StepIdx {
+    const StepCoef *coef; // per-iteration coefficients of this call
+    const int *base;      // device counter: index of the chunk's first iteration
+    int local;            // iteration within the chunk
+};
+
+enum { ZM_RT_PRO = 0, ZM_RT_MID, ZM_RT_EPI, ZM_IT_PRO, ZM_IT_MID };
+
+// ---------------------------------------------------------------------------
+// X pencils
+// ---------------------------------------------------------------------------
+template <class R, int NX, bool KIN>
+__global__ void __launch_bounds__(256, 4)
+    k2_x(cplx<R> *__restrict__ psi, cplx<R> *__restrict__ S, const R *__restrict__ vk,
+         const cplx<R> *__restrict__ ex, const cplx<R> *__restrict__ ey, const cplx<R> *__restrict__ ez,
+         R inv_hi, R inv_lo, const double *__restrict__ divisor, double dip_scale, int ny, int nz,
+         int nblk_kin, Twid tk, Twid td) {
+    using C          = cplx<R>;
+    constexpr int NT = 256;
+    const int tid    = threadIdx.x;
+    C *b0            = reinterpret_cast<C *>(g_smem);
+    if (KIN && (int)blockIdx.x < nblk_kin) {
+        constexpr int CK = tile_lines<R, NX>();
+        const int cols   = ny * nz;
+        const int c0     = blockIdx.x * CK;
+        const int cnt    = min(CK, cols - c0);
+#pragma unroll 4
+        for (int e = tid; e < CK * NX; e += NT) {
+            const int i = e / CK, b = e % CK;
+            b0[b + i * CK] = b < cnt ? psi[(size_t)i * cols + c0 + b] : C{(R)0, (R)0};
+        }
+        __syncthreads();
+        ct_fft_ip<-1, R, NX, CK, CK, NT>(b0, (const C *)tk.tw, (const C *)tk.lo, tid);
+        C *r1 = b0;
+        {
+            // each thread keeps one column b for all its elements when CK | NT
+            for (int e = tid; e < CK * NX; e += NT) {
+                const int i = e / CK, b = e % CK;
+                const int c = c0 + b, j = c / nz, k = c - j * nz;
+                if (b < cnt) {
+                    const C w = combine_wm1(__ldg(&ex[i]), __ldg(&ey[j]), __ldg(&ez[k]));
+                    const C v = apply_wm1(r1[b + i * CK], w);
+                    r1[b + i * CK] = C{fma(v.x, inv_hi, v.x * inv_lo), fma(v.y, inv_hi, v.y * inv_lo)};
+                }
+            }
+        }
+        __syncthreads();
+        ct_fft_ip<+1, R, NX, CK, CK, NT>(b0, (const C *)tk.tw, (const C *)tk.lo, tid);
+#pragma unroll 4
+        for (int e = tid; e < CK * NX; e += NT) {
+            const int i = e / CK, b = e % CK;
+            if (b < cnt)
+                psi[(size_t)i * cols + c0 + b] = b0[b + i * CK];
+        }
+        return;
+    }
+    constexpr int L  = 2 * NX;
+    constexpr int CD = tile_lines<R, L>();
+    const int cols   = 2 * ny * nz;
+    const int c0     = ((int)blockIdx.x - (KIN ? nblk_kin : 0)) * CD;
+    const int cnt    = min(CD, cols - c0);
+#pragma unroll 4
+    for (int e = tid; e < CD * NX; e += NT) {
+        const int i = e / CD, b = e % CD;
+        b0[b + i * CD]        = b < cnt ? S[(size_t)i * cols + c0 + b] : C{(R)0, (R)0};
+        b0[b + (i + NX) * CD] = C{(R)0, (R)0};
+    }
+    __syncthreads();
+    ct_fft_ip<-1, R, L, CD, CD, NT>(b0, (const C *)td.tw, (const C *)td.lo, tid);
+    C *r1 = b0;
+    // V_dd(k) * scale; scale = 1/(8N) (C2R normalisation) and, for imaginary
+    // time, 1/xnorma (the spectrum was built from the unnormalised psi)
+    const R scale = (R)(divisor ? dip_scale / divisor[0] : dip_scale);
+    for (int e = tid; e < CD * L; e += NT) {
+        const int t = e / CD, b = e % CD;
+        const int c = c0 + b, ky = c / nz, kz = c - ky * nz;
+        const int ix = t <= NX ? t : L - t;
+        const int iy = ky <= ny ? ky : 2 * ny - ky;
+        const R v    = (b < cnt) ? __ldg(&vk[((size_t)ix * (ny + 1) + iy) * nz + kz]) * scale : (R)0;
+        r1[b + t * CD] = cscale(r1[b + t * CD], v);
+    }
+    __syncthreads();
+    ct_fft_ip<+1, R, L, CD, CD, NT>(b0, (const C *)td.tw, (const C *)td.lo, tid);
+#pragma unroll 4
+    for (int e = tid; e < CD * NX; e += NT) {
+        const int i = e / CD, b = e % CD;
+        if (b < cnt)
+            S[(size_t)i * cols + c0 + b] = b0[b + i * CD];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Y lines (one x plane per blockIdx.y; z-column tiles along blockIdx.x)
+// ---------------------------------------------------------------------------
+template <class R, int NY, int SIGN, bool KIN>
+__global__ void __launch_bounds__(256, 4)
+    k2_y(cplx<R> *__restrict__ psi, cplx<R> *__restrict__ S, int nz, int nblk_kin, Twid tk, Twid td) {
+    using C          = cplx<R>;
+    constexpr int NT = 256;
+    const int tid    = threadIdx.x;
+    const int i      = blockIdx.y;
+    C *b0            = reinterpret_cast<C *>(g_smem);
+    if (KIN && (int)blockIdx.x < nblk_kin) {
+        constexpr int CY = tile_lines<R, NY>() < 16 ? tile_lines<R, NY>() : 16;
+        const int k0     = blockIdx.x * CY;
+        const int cnt    = min(CY, nz - k0);
+        C *plane         = psi + (size_t)i * NY * nz;
+#pragma unroll 4
+        for (int e = tid; e < CY * NY; e += NT) {
+            const int j = e / CY, b = e % CY;
+            b0[b + j * CY] = b < cnt ? plane[(size_t)j * nz + k0 + b] : C{(R)0, (R)0};
+        }
+        __syncthreads();
+        ct_fft_ip<SIGN, R, NY, CY, CY, NT>(b0, (const C *)tk.tw, (const C *)tk.lo, tid);
+#pragma unroll 4
+        for (int e = tid; e < CY * NY; e += NT) {
+            const int j = e / CY, b = e % CY;
+            if (b < cnt)
+                plane[(size_t)j * nz + k0 + b] = b0[b + j * CY];
+        }
+        return;
+    }
+    constexpr int L  = 2 * NY;
+    constexpr int CD = tile_lines<R, L>() < 16 ? tile_lines<R, L>() : 16;
+    const int k0     = ((int)blockIdx.x - (KIN ? nblk_kin : 0)) * CD;
+    const int cnt    = min(CD, nz - k0);
+    C *plane         = S + (size_t)i * L * nz;
+    if (SIGN < 0) {
+#pragma unroll 4
+        for (int e = tid; e < CD * NY; e += NT) {
+            const int j = e / CD, b = e % CD;
+            b0[b + j * CD]        = b < cnt ? plane[(size_t)j * nz + k0 + b] : C{(R)0, (R)0};
+            b0[b + (j + NY) * CD] = C{(R)0, (R)0};
+        }
+    } else {
+#pragma unroll 4
+        for (int e = tid; e < CD * L; e += NT) {
+            const int j = e / CD, b = e % CD;
+            b0[b + j * CD] = b < cnt ? plane[(size_t)j * nz + k0 + b] : C{(R)0, (R)0};
+        }
+    }
+    __syncthreads();
+    ct_fft_ip<SIGN, R, L, CD, CD, NT>(b0, (const C *)td.tw, (const C *)td.lo, tid);
+    const int rows_out = SIGN < 0 ? L : NY;
+    for (int e = tid; e < CD * rows_out; e += NT) {
+        const int j = e / CD, b = e % CD;
+        if (b < cnt)
+            plane[(size_t)j * nz + k0 + b] = b0[b + j * CD];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Z rows
+// ---------------------------------------------------------------------------
+struct ZArgs {
+    // fields
+    void *psi_in;        // kinetic spectrum (RT), or psi (RT_PRO, IT)
+    void *psi_out;       // RT: same as psi_in; IT: the next psi buffer
+    const void *bnd;     // IT: boundary values (last loaded psi)
+    void *S;             // dipolar spectrum
+    const void *V;
+    void *phi;
+    // norms (IT)
+    double *norm_state;  // [0] xnorma, [1] divisor of psi_in (read), both written by the last CTA
+    double *partial;     // per-CTA partial sums of |psi_out|^2
+    unsigned *ticket;    // CTA completion counter (reset by the last CTA)
+    int *status;
+    double dV;
+    // coefficients
+    StepIdx step;
+    double half_dt, cdd, w_atoms;
+    double cx, cy, cz, dtau; // IT stencil
+    int nx, ny;
+};
+
+template <class R, int NZ, int MODE>
+__global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
+    using C          = cplx<R>;
+    constexpr int NT = 256;
+    constexpr int RW = 32;          // rows per CTA
+    constexpr int NP = RW / 2;      // row pairs for the real transforms
+    constexpr int LD = 2 * NZ;      // dipolar line length
+    constexpr int TK = RW + 1;      // tile strides (odd: transposing loads avoid bank conflicts)
+    constexpr int TD = NP + 1;
+    constexpr bool RT      = MODE <= ZM_RT_EPI;
+    constexpr bool HAS_INV = (MODE == ZM_RT_MID || MODE == ZM_RT_EPI || MODE == ZM_IT_MID);
+    constexpr bool HAS_FWD = (MODE != ZM_RT_EPI);
+    const int tid          = threadIdx.x;
+    const int nx = a.nx, ny = a.ny;
+    const int rows = nx * ny;
+    const int r0   = blockIdx.x * RW;
+
+    C *kb0  = reinterpret_cast<C *>(g_smem); // kinetic tile [k][row]
+    C *db0  = kb0 + TK * NZ;                 // dipolar pair tile [m][pair]
+    R *phis = reinterpret_cast<R *>(db0 + TD * LD); // phi, then rho, [k][row]
+    __shared__ double red[8];
+
+    const C *S_in = reinterpret_cast<const C *>(a.S);
+    C *S_out      = reinterpret_cast<C *>(a.S);
+
+    // ---- phi: dipolar C2R of the row pairs -------------------------------
+    if (HAS_INV) {
+        for (int e = tid; e < NP * LD; e += NT) {
+            const int p = e % NP, m = e / NP;
+            const int ra = r0 + 2 * p, rb = ra + 1;
+            C z = C{(R)0, (R)0};
+            if (m > 0 && ra < rows) {
+                const int ia = ra / ny, ja = ra - ia * ny;
+                const int mm = m <= NZ ? m : LD - m;
+                const C xa   = S_in[((size_t)ia * 2 * ny + ja) * NZ + (mm - 1)];
+                C xb         = C{(R)0, (R)0};
+                if (rb < rows) {
+                    const int ib = rb / ny, jb = rb - ib * ny;
+                    xb           = S_in[((size_t)ib * 2 * ny + jb) * NZ + (mm - 1)];
+                }
+                if (m == NZ)
+                    z = C{xa.x, xb.x}; // self-conjugate bin: real parts only
+                else if (m < NZ)
+                    z = C{xa.x - xb.y, xa.y + xb.x};   // xa + i xb
+                else
+                    z = C{xa.x + xb.y, xb.x - xa.y};   // conj(xa) + i conj(xb)
+            }
+            db0[p + m * TD] = z;
+        }
+        __syncthreads();
+        ct_fft_ip<+1, R, LD, NP, TD, NT>(db0, (const C *)td.tw, (const C *)td.lo, tid);
+        const C *r = db0;
+        R *phi_g = reinterpret_cast<R *>(a.phi);
+        for (int e = tid; e < RW * NZ; e += NT) {
+            const int row = e / NZ, k = e % NZ; // coalesced store along k
+            const int p = row >> 1;
+            const C zz  = r[p + k * TD];
+            const R v   = (row & 1) ? zz.y : zz.x;
+            phis[row + k * TK] = v;
+            if (r0 + row < rows)
+                phi_g[(size_t)(r0 + row) * NZ + k] = v;
+        }
+        __syncthreads();
+    } else if (RT) {
+        // prologue: phi from the previous calc_fi3d
+        const R *phi_g = reinterpret_cast<const R *>(a.phi);
+        for (int e = tid; e < RW * NZ; e += NT) {
+            const int row = e / NZ, k = e % NZ;
+            phis[row + k * TK] = (r0 + row < rows) ? phi_g[(size_t)(r0 + row) * NZ + k] : (R)0;
+        }
+    }
+
+    // ---- psi for the physics step -----------------------------------------
+    C *kt = kb0; // tile holding psi in real space, [k][row]
+    if (RT) {
+        const C *pin = reinterpret_cast<const C *>(a.psi_in);
+        for (int e = tid; e < RW * NZ; e += NT) {
+            const int row = e / NZ, k = e % NZ;
+            kb0[row + k * TK] = (r0 + row < rows) ? pin[(size_t)(r0 + row) * NZ + k] : C{(R)0, (R)0};
+        }
+        __syncthreads();
+        if (MODE != ZM_RT_PRO)
+            ct_fft_ip<+1, R, NZ, RW, TK, NT>(kb0, (const C *)tk.tw, (const C *)tk.lo, tid);
+    }
+
+    double acc = 0.0;
+    if (RT) {
+        // merged potential half steps: theta = -dt/2 [cV (V + cdd phi) + g3 |psi|^2 + gw |psi|^3]
+        R cV, g3, gw;
+        {
+            const int base = *a.step.base + a.step.local;
+            const StepCoef c0 = a.step.coef[base];
+            if (MODE == ZM_RT_MID) {
+                const StepCoef c1 = a.step.coef[base + 1];
+                cV = (R)2;
+                g3 = (R)(c0.g3w + c1.g3w);
+                gw = (R)(c0.gw15 + c1.gw15);
+            } else {
+                cV = (R)1;
+                g3 = (R)c0.g3w;
+                gw = (R)c0.gw15;
+            }
+        }
+        const R *Vg   = reinterpret_cast<const R *>(a.V);
+        const R hdt   = (R)a.half_dt, cdd = (R)a.cdd, wat = (R)a.w_atoms;
+        for (int e = tid; e < RW * NZ; e += NT) {
+            const int row = e / NZ, k = e % NZ;
+            const int rr  = r0 + row;
+            if (rr >= rows)
+                continue;
+            const int i = rr / ny, j = rr - i * ny;
+            C p         = kt[row + k * TK];
+            if (i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < NZ - 1) {
+                const R dens  = p.x * p.x + p.y * p.y;
+                const R am    = sqrt(dens);
+                const R total = cV * (Vg[(size_t)rr * NZ + k] + cdd * phis[row + k * TK]) + g3 * dens +
+                                gw * (am * am * am);
+                R s, c;
+                sincos_r<R>((R)-0.5 * hdt * total, &s, &c);
+                p = apply_wm1(p, C{(R)-2 * s * s, (R)2 * s * c});
+                kt[row + k * TK] = p;
+            }
+            // rho for the next dipolar spectrum (stored in the phi tile)
+            phis[row + k * TK] = wat * (p.x * p.x + p.y * p.y);
+        }
+        __syncthreads();
+        if (MODE == ZM_RT_EPI) {
+            C *pout = reinterpret_cast<C *>(a.psi_out);
+            for (int e = tid; e < RW * NZ; e += NT) {
+                const int row = e / NZ, k = e % NZ;
+                if (r0 + row < rows)
+                    pout[(size_t)(r0 + row) * NZ + k] = kt[row + k * TK];
+            }
+            return;
+        }
+        // kinetic forward z
+        ct_fft_ip<-1, R, NZ, RW, TK, NT>(kb0, (const C *)tk.tw, (const C *)tk.lo, tid);
+        const C *kf = kb0;
+        C *pout     = reinterpret_cast<C *>(a.psi_out);
+        for (int e = tid; e < RW * NZ; e += NT) {
+            const int row = e / NZ, k = e % NZ;
+            if (r0 + row < rows)
+                pout[(size_t)(r0 + row) * NZ + k] = kf[row + k * TK];
+        }
+    } else {
+        // imaginary time: psi_in / sqrt(divisor)
+        const C *pin  = reinterpret_cast<const C *>(a.psi_in);
+        C *pout       = reinterpret_cast<C *>(a.psi_out);
+        const C *bnd  = reinterpret_cast<const C *>(a.bnd);
+        const R sc    = (R)(1.0 / sqrt(a.norm_state[1]));
+        const R wat   = (R)a.w_atoms;
+        const size_t plane = (size_t)ny * NZ;
+        if (MODE == ZM_IT_PRO) {
+            for (int e = tid; e < RW * NZ; e += NT) {
+                const int row = e / NZ, k = e % NZ;
+                const int rr  = r0 + row;
+                R rho         = (R)0;
+                if (rr < rows) {
+                    const C p = pin[(size_t)rr * NZ + k];
+                    rho       = wat * (p.x * p.x + p.y * p.y);
+                }
+                phis[row + k * TK] = rho;
+            }
+        } else {
+            const StepCoef cf = a.step.coef[0];
+            const R g3w = (R)cf.g3w, gw15 = (R)cf.gw15;
+            const R *Vg = reinterpret_cast<const R *>(a.V);
+            const R cx = (R)a.cx, cy = (R)a.cy, cz = (R)a.cz, dtau = (R)a.dtau, cdd = (R)a.cdd;
+            for (int e = tid; e < RW * NZ; e += NT) {
+                const int row = e / NZ, k = e % NZ;
+                const int rr  = r0 + row;
+                R rho         = (R)0;
+                if (rr < rows) {
+                    const int i = rr / ny, j = rr - i * ny;
+                    const size_t q = (size_t)rr * NZ + k;
+                    C o;
+                    if (i < 1 || i >= nx - 1 || j < 1 || j >= ny - 1 || k < 1 || k >= NZ - 1) {
+                        o = bnd[q];
+                    } else {
+                        const C c0 = cscale(pin[q], sc);
+                        const C xm = cscale(pin[q - plane], sc), xp = cscale(pin[q + plane], sc);
+                        const C ym = cscale(pin[q - NZ], sc), yp = cscale(pin[q + NZ], sc);
+                        const C zm = cscale(pin[q - 1], sc), zp = cscale(pin[q + 1], sc);
+                        const R vv   = Vg[q] + cdd * phis[row + k * TK];
+                        const R dens = c0.x * c0.x + c0.y * c0.y;
+                        const R am   = sqrt(dens);
+                        const R nl   = g3w * dens + gw15 * (am * am * am);
+                        const R lr   = cx * ((xm.x + xp.x) - 2 * c0.x) - cy * ((ym.x + yp.x) - 2 * c0.x) -
+                                     cz * ((zm.x + zp.x) - 2 * c0.x) + c0.x * vv + nl * c0.x;
+                        const R li = cx * ((xm.y + xp.y) - 2 * c0.y) - cy * ((ym.y + yp.y) - 2 * c0.y) -
+                                     cz * ((zm.y + zp.y) - 2 * c0.y) + c0.y * vv + nl * c0.y;
+                        o = C{c0.x - dtau * lr, c0.y - dtau * li};
+                    }
+                    pout[q] = o;
+                    acc += (double)o.x * o.x + (double)o.y * o.y;
+                    rho = wat * (o.x * o.x + o.y * o.y);
+                }
+                phis[row + k * TK] = rho;
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- dipolar R2C of rho (row pairs) -> spectrum -------------------------
+    if (HAS_FWD) {
+        for (int e = tid; e < NP * LD; e += NT) {
+            const int p = e % NP, m = e / NP;
+            C z         = C{(R)0, (R)0};
+            if (m < NZ)
+                z = C{phis[2 * p + m * TK], phis[2 * p + 1 + m * TK]};
+            db0[p + m * TD] = z;
+        }
+        __syncthreads();
+        ct_fft_ip<-1, R, LD, NP, TD, NT>(db0, (const C *)td.tw, (const C *)td.lo, tid);
+        const C *r = db0;
+        for (int e = tid; e < RW * NZ; e += NT) {
+            const int row = e / NZ, m = e % NZ + 1; // bins 1..NZ
+            const int rr  = r0 + row;
+            if (rr >= rows)
+                continue;
+            const int p  = row >> 1;
+            const C zm   = r[p + m * TD];
+            const C zc   = r[p + (LD - m) * TD];
+            C x;
+            if ((row & 1) == 0)
+                x = C{(R)0.5 * (zm.x + zc.x), (R)0.5 * (zm.y - zc.y)};   // (Z_m + conj(Z_{L-m}))/2
+            else
+                x = C{(R)0.5 * (zm.y + zc.y), (R)0.5 * (zc.x - zm.x)};   // (Z_m - conj(Z_{L-m}))/(2i)
+            const int i = rr / ny, j = rr - i * ny;
+            S_out[((size_t)i * 2 * ny + j) * NZ + (m - 1)] = x;
+        }
+    }
+
+    // ---- norm of psi' (imaginary time): deterministic two-level reduction ---
+    if (MODE == ZM_IT_MID) {
+        for (int off = 16; off > 0; off >>= 1)
+            acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if ((tid & 31) == 0)
+            red[tid >> 5] = acc;
+        __syncthreads();
+        __shared__ bool last;
+        if (tid == 0) {
+            double v = 0;
+            for (int w = 0; w < NT / 32; ++w)
+                v += red[w];
+            a.partial[blockIdx.x] = v;
+            __threadfence();
+            const unsigned t = atomicAdd(a.ticket, 1u);
+            last             = (t == gridDim.x - 1);
+        }
+        __syncthreads();
+        if (last) {
+            __threadfence();
+            double v = 0;
+            for (int b = tid; b < (int)gridDim.x; b += NT)
+                v += ((volatile double *)a.partial)[b];
+            for (int off = 16; off > 0; off >>= 1)
+                v += __shfl_down_sync(0xffffffffu, v, off);
+            if ((tid & 31) == 0)
+                red[tid >> 5] = v;
+            __syncthreads();
+            if (tid == 0) {
+                double x = 0;
+                for (int w = 0; w < NT / 32; ++w)
+                    x += red[w];
+                x *= a.dV;
+                a.norm_state[0] = x;
+                a.norm_state[1] = x;
+                if (!(x > 0.0) || !isfinite(x))
+                    a.status[0] = 1;
+                *a.ticket = 0u;
+            }
+        }
+    }
+}
+
+// Shared memory of k2_z<R, NZ, *>.
+template <class R, int NZ> constexpr size_t z_smem() {
+    return sizeof(cplx<R>) * (33 * NZ + 17 * 2 * NZ) + sizeof(R) * 33 * NZ;
+}
+
+} // namespace gpe

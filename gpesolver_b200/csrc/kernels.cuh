@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(256)
         const int c = c0 + b, j = c / nz, k = c - j * nz;
         const C w   = combine_wm1(__ldg(&ex[i]), __ldg(&ey[j]), __ldg(&ez[k]));
         const C v   = apply_wm1(res[i * TB + b], w);
-        res[i * TB + b] = C{fma(v.x, inv_lo, v.x * inv_hi), fma(v.y, inv_lo, v.y * inv_hi)};
+        res[i * TB + b] = C{fma(v.x, inv_hi, v.x * inv_lo), fma(v.y, inv_hi, v.y * inv_lo)};
     }
     __syncthreads();
     C *res2 = block_fft<+1, R>(res, other, ln, cnt, 1, TB, threadIdx.x, blockDim.x);

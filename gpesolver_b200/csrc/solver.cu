@@ -6,6 +6,7 @@
 // waits where the reference's interface returns a value (norm, energies,
 // exported fields).
 #include "../../include/gpe_b200.h"
+#include "fused.cuh"
 #include "kernels.cuh"
 #include "plan.hpp"
 
@@ -197,10 +198,20 @@ template <class R> class Solver final : public SolverBase {
         epartial.alloc(5 * (size_t)nblk_elem);
 
         build_tables();
+        fused = std::is_same<R, float>::value && p.schedule == 0 && fused_dim_xy(nx) &&
+                fused_dim_xy(ny) && fused_dim_z(nz);
+        if (fused) {
+            S2.alloc((size_t)nx * 2 * ny * nz);
+            zpartial.alloc((size_t)(nx * ny + 31) / 32);
+            ticket.alloc(1);
+            build_vk2();
+        }
         set_coeffs(p.ggp11, p.gamma);
         set_divisor_one();
         GPE_CUDA(cudaStreamSynchronize(cur));
         set_smem_attrs();
+        if (fused)
+            set_fused_attrs();
     }
 
     ~Solver() override {
@@ -346,6 +357,12 @@ template <class R> class Solver final : public SolverBase {
             return;
         if (!lazy)
             set_divisor_one();
+        if (fused) {
+            fused_imag(k);
+            lazy = true;
+            check_status();
+            return;
+        }
         const int CH = kItChunk;
         long done    = 0;
         while (k - done >= CH) {
@@ -379,6 +396,11 @@ template <class R> class Solver final : public SolverBase {
         GPE_CUDA(cudaMemcpyAsync(coef_dev.p, coef_host, sizeof(StepCoef) * k, cudaMemcpyHostToDevice, cur));
         GPE_CUDA(cudaEventRecord(coef_event, cur));
         GPE_CUDA(cudaMemsetAsync(iter_base.p, 0, sizeof(int), cur));
+        if (fused) {
+            fused_real(k);
+            check_status();
+            return;
+        }
         const int CH = kRtChunk;
         long done    = 0;
         while (k - done >= CH) {
@@ -400,6 +422,15 @@ template <class R> class Solver final : public SolverBase {
         save_A.alloc(A.n);
         GPE_CUDA(cudaMemcpyAsync(save_psi.p, psi.p, sizeof(C) * N, cudaMemcpyDeviceToDevice, cur));
         GPE_CUDA(cudaMemcpyAsync(save_A.p, A.p, sizeof(C) * A.n, cudaMemcpyDeviceToDevice, cur));
+        if (which == GPE_K_F_Z) {
+            // the merged phase reads the coefficients of two consecutive iterations
+            ensure_coef_capacity(2);
+            GPE_CUDA(cudaEventSynchronize(coef_event));
+            coef_host[0] = coef_host[1] = host_coef;
+            GPE_CUDA(cudaMemcpyAsync(coef_dev.p, coef_host, 2 * sizeof(StepCoef), cudaMemcpyHostToDevice, cur));
+            GPE_CUDA(cudaEventRecord(coef_event, cur));
+            GPE_CUDA(cudaMemsetAsync(iter_base.p, 0, sizeof(int), cur));
+        }
         cudaEvent_t e0, e1;
         GPE_CUDA(cudaEventCreate(&e0));
         GPE_CUDA(cudaEventCreate(&e1));
@@ -463,6 +494,29 @@ template <class R> class Solver final : public SolverBase {
                 enqueue_phase(cur, cur_coef.p, iter_zero.p, 0);
                 b = 2 * F + 2 * Rb;
                 break;
+            case GPE_K_F_X:
+            case GPE_K_F_YINV:
+            case GPE_K_F_Z:
+            case GPE_K_F_YFWD: {
+                if (!fused)
+                    throw Error(GPE_ERR_STATE, "the fused pipeline is not available for this grid");
+                const double S2b = (double)sizeof(C) * nx * 2 * ny * nz;
+                const double S2h = (double)sizeof(C) * nx * ny * nz;
+                if (which == GPE_K_F_X) {
+                    f_x(cur, true, nullptr);
+                    b = 2 * F + 2 * S2h; // kinetic R+W; dipolar reads and writes nx of 2nx planes
+                } else if (which == GPE_K_F_YINV) {
+                    f_y<+1>(cur, true);
+                    b = 2 * F + S2b + S2h;
+                } else if (which == GPE_K_F_YFWD) {
+                    f_y<-1>(cur, true);
+                    b = 2 * F + S2h + S2b;
+                } else {
+                    f_z<ZM_RT_MID>(cur, psi.p, psi.p, coef_dev.p, 0);
+                    b = 2 * F + 2 * S2h + Rb + Rb; // psi R+W, spectrum R+W, V read, phi write
+                }
+                break;
+            }
             default:
                 enqueue_it_update(cur, psi.p, psii.p);
                 b = 2 * F + 2 * Rb;
@@ -487,6 +541,252 @@ template <class R> class Solver final : public SolverBase {
     }
 
   private:
+    // ---- fused pipeline ---------------------------------------------------
+    static bool fused_dim_xy(int n) { return n == 32 || n == 64 || n == 96 || n == 128 || n == 256; }
+    static bool fused_dim_z(int n) { return n == 8 || n == 16 || n == 24 || n == 32 || n == 64; }
+
+    // V_dd(k) for kz = 1..nz (the kz = 0 plane is identically zero), reduced by
+    // |kx|, |ky| symmetry, FP64 as fftw_poisson_solver.cpp:12-49.
+    void build_vk2() {
+        const int px = 2 * nx, py = 2 * ny, pz = 2 * nz;
+        const double dkx = 2. * M_PI / (px * P.dx), dky = 2. * M_PI / (py * P.dy),
+                     dkz = 2. * M_PI / (pz * P.dz);
+        std::vector<R> t((size_t)(nx + 1) * (ny + 1) * nz);
+        for (int i = 0; i <= nx; ++i) {
+            const double kxv = i * dkx;
+            for (int j = 0; j <= ny; ++j) {
+                const double kyv = j * dky;
+                for (int k = 1; k <= nz; ++k) {
+                    const double kzv = k * dkz;
+                    const double k2  = kxv * kxv + kyv * kyv + kzv * kzv;
+                    t[((size_t)i * (ny + 1) + j) * nz + (k - 1)] = (R)((k2 > 1e-30) ? (kzv * kzv / k2) : 0.0);
+                }
+            }
+        }
+        vk2.alloc(t.size());
+        GPE_CUDA(cudaMemcpy(vk2.p, t.data(), sizeof(R) * t.size(), cudaMemcpyHostToDevice));
+    }
+
+    static Twid twid(const Line &l) { return Twid{l.plan.tw, l.plan.twlo}; }
+
+    template <int N> static constexpr size_t x_smem(bool kin) {
+        const size_t k = kin ? (size_t)tile_lines<R, N>() * N : 0;
+        const size_t d = (size_t)tile_lines<R, 2 * N>() * 2 * N;
+        return sizeof(C) * (k > d ? k : d);
+    }
+    template <int N> static constexpr int y_ck() { return tile_lines<R, N>() < 16 ? tile_lines<R, N>() : 16; }
+    template <int N> static constexpr int y_cd() {
+        return tile_lines<R, 2 * N>() < 16 ? tile_lines<R, 2 * N>() : 16;
+    }
+    template <int N> static constexpr size_t y_smem(bool kin) {
+        const size_t k = kin ? (size_t)y_ck<N>() * N : 0;
+        const size_t d = (size_t)y_cd<N>() * 2 * N;
+        return sizeof(C) * (k > d ? k : d);
+    }
+
+#define GPE_XY_CASES(M) M(32) M(64) M(96) M(128) M(256)
+#define GPE_Z_CASES(M) M(8) M(16) M(24) M(32) M(64)
+
+    void set_fused_attrs() {
+        if constexpr (std::is_same<R, float>::value) {
+            auto set = [](const void *f, size_t bytes) {
+                if (bytes > 48 * 1024)
+                    GPE_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+            };
+#define GPE_SETX(N)                                                                                \
+    if (nx == N) {                                                                                 \
+        set((const void *)k2_x<R, N, true>, x_smem<N>(true));                                       \
+        set((const void *)k2_x<R, N, false>, x_smem<N>(false));                                     \
+    }
+#define GPE_SETY(N)                                                                                \
+    if (ny == N) {                                                                                 \
+        set((const void *)k2_y<R, N, -1, true>, y_smem<N>(true));                                   \
+        set((const void *)k2_y<R, N, +1, true>, y_smem<N>(true));                                   \
+        set((const void *)k2_y<R, N, -1, false>, y_smem<N>(false));                                 \
+        set((const void *)k2_y<R, N, +1, false>, y_smem<N>(false));                                 \
+    }
+#define GPE_SETZ(N)                                                                                \
+    if (nz == N) {                                                                                 \
+        set((const void *)k2_z<R, N, ZM_RT_PRO>, z_smem<R, N>());                                   \
+        set((const void *)k2_z<R, N, ZM_RT_MID>, z_smem<R, N>());                                   \
+        set((const void *)k2_z<R, N, ZM_RT_EPI>, z_smem<R, N>());                                   \
+        set((const void *)k2_z<R, N, ZM_IT_PRO>, z_smem<R, N>());                                   \
+        set((const void *)k2_z<R, N, ZM_IT_MID>, z_smem<R, N>());                                   \
+    }
+            GPE_XY_CASES(GPE_SETX)
+            GPE_XY_CASES(GPE_SETY)
+            GPE_Z_CASES(GPE_SETZ)
+#undef GPE_SETX
+#undef GPE_SETY
+#undef GPE_SETZ
+        }
+    }
+
+    void f_x(cudaStream_t s, bool kin, const double *divisor) {
+        if constexpr (std::is_same<R, float>::value) {
+            const double dscale = 1.0 / (8.0 * (double)N);
+#define GPE_LX(NN)                                                                                 \
+    if (nx == NN) {                                                                                \
+        constexpr int CK = tile_lines<R, NN>(), CD = tile_lines<R, 2 * NN>();                     \
+        const int nk = kin ? (ny * nz + CK - 1) / CK : 0;                                          \
+        const int nd = (2 * ny * nz + CD - 1) / CD;                                                \
+        if (kin)                                                                                   \
+            launch(k2_x<R, NN, true>, nk + nd, 256, x_smem<NN>(true), s, psi.p, S2.p, (const R *)vk2.p, \
+                   (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, divisor, dscale, \
+                   ny, nz, nk, twid(kx), twid(dx));                                                \
+        else                                                                                       \
+            launch(k2_x<R, NN, false>, nd, 256, x_smem<NN>(false), s, psi.p, S2.p, (const R *)vk2.p, \
+                   (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, divisor, dscale, \
+                   ny, nz, 0, twid(kx), twid(dx));                                                 \
+    }
+            GPE_XY_CASES(GPE_LX)
+#undef GPE_LX
+        }
+    }
+
+    template <int SIGN> void f_y(cudaStream_t s, bool kin) {
+        if constexpr (std::is_same<R, float>::value) {
+#define GPE_LY(NN)                                                                                 \
+    if (ny == NN) {                                                                                \
+        constexpr int CK = y_ck<NN>(), CD = y_cd<NN>();                                            \
+        const int nk = kin ? (nz + CK - 1) / CK : 0;                                               \
+        const int nd = (nz + CD - 1) / CD;                                                         \
+        if (kin)                                                                                   \
+            launch(k2_y<R, NN, SIGN, true>, dim3(nk + nd, nx), 256, y_smem<NN>(true), s, psi.p, S2.p, \
+                   nz, nk, twid(ky), twid(dy));                                                    \
+        else                                                                                       \
+            launch(k2_y<R, NN, SIGN, false>, dim3(nd, nx), 256, y_smem<NN>(false), s, psi.p, S2.p, nz, \
+                   0, twid(ky), twid(dy));                                                         \
+    }
+            GPE_XY_CASES(GPE_LY)
+#undef GPE_LY
+        }
+    }
+
+    template <int MODE> void f_z(cudaStream_t s, C *pin, C *pout, const StepCoef *coef, int local) {
+        if constexpr (std::is_same<R, float>::value) {
+            ZArgs a{};
+            a.psi_in     = pin;
+            a.psi_out    = pout;
+            a.bnd        = bnd.p;
+            a.S          = S2.p;
+            a.V          = V.p;
+            a.phi        = phi.p;
+            a.norm_state = norm_state.p;
+            a.partial    = zpartial.p;
+            a.ticket     = ticket.p;
+            a.status     = status.p;
+            a.dV         = P.dx * P.dy * P.dz;
+            a.step       = StepIdx{coef, iter_base.p, local};
+            a.half_dt    = P.real_time_dt / 2.;
+            a.cdd        = P.cdd;
+            a.w_atoms    = P.n_atoms;
+            a.cx         = -0.5 / (P.m * P.dx * P.dx);
+            a.cy         = 0.5 / (P.m * P.dy * P.dy);
+            a.cz         = 0.5 / (P.m * P.dz * P.dz);
+            a.dtau       = P.imag_time_dt;
+            a.nx         = nx;
+            a.ny         = ny;
+            const int grid = (nx * ny + 31) / 32;
+#define GPE_LZ(NN)                                                                                 \
+    if (nz == NN)                                                                                  \
+        launch(k2_z<R, NN, MODE>, grid, 256, z_smem<R, NN>(), s, a, twid(kz), twid(dz));
+            GPE_Z_CASES(GPE_LZ)
+#undef GPE_LZ
+        }
+    }
+
+    // kind 10: RT prologue; 11: C mid RT iterations; 12: `count` mid + the last;
+    // kind 20: IT prologue; 21: `count` IT iterations.
+    void capture_fused(int kind, int count) {
+        cudaStream_t s = cap_stream;
+        if (kind == 10) {
+            f_z<ZM_RT_PRO>(s, psi.p, psi.p, coef_dev.p, 0);
+            f_y<-1>(s, true);
+        } else if (kind == 11 || kind == 12) {
+            for (int t = 0; t < count; ++t) {
+                f_x(s, true, nullptr);
+                f_y<+1>(s, true);
+                f_z<ZM_RT_MID>(s, psi.p, psi.p, coef_dev.p, t);
+                f_y<-1>(s, true);
+            }
+            if (kind == 12) {
+                f_x(s, true, nullptr);
+                f_y<+1>(s, true);
+                f_z<ZM_RT_EPI>(s, psi.p, psi.p, coef_dev.p, count);
+            } else {
+                launch(k_advance, 1, 1, 0, s, iter_base.p, count);
+            }
+        } else if (kind == 20) {
+            f_z<ZM_IT_PRO>(s, psi.p, psi.p, cur_coef.p, 0);
+            f_y<-1>(s, false);
+        } else {
+            C *a = psi.p, *b = psii.p;
+            for (int t = 0; t < count; ++t) {
+                f_x(s, false, norm_state.p + 1);
+                f_y<+1>(s, false);
+                f_z<ZM_IT_MID>(s, a, b, cur_coef.p, 0);
+                f_y<-1>(s, false);
+                std::swap(a, b);
+            }
+        }
+    }
+
+    void run_fused_graph(int kind, int count) {
+        auto key = std::make_tuple(kind, count, (const void *)psi.p);
+        auto it  = graphs.find(key);
+        if (it == graphs.end()) {
+            const long long before = n_launch;
+            GPE_CUDA(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                capture_fused(kind, count);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(cap_stream, &g);
+                if (g)
+                    cudaGraphDestroy(g);
+                throw;
+            }
+            cudaGraph_t g;
+            GPE_CUDA(cudaStreamEndCapture(cap_stream, &g));
+            cudaGraphExec_t ge;
+            GPE_CUDA(cudaGraphInstantiate(&ge, g, 0));
+            cudaGraphDestroy(g);
+            graphs[key]      = ge;
+            graph_nodes[key] = (int)(n_launch - before);
+            n_launch         = before;
+            it               = graphs.find(key);
+        }
+        GPE_CUDA(cudaGraphLaunch(it->second, cur));
+        n_launch += graph_nodes[key];
+        if (kind == 21 && (count & 1))
+            std::swap(psi.p, psii.p);
+    }
+
+    void fused_real(long k) {
+        run_fused_graph(10, 0);
+        const long mid = k - 1;
+        const int CH   = kRtChunk;
+        long done      = 0;
+        while (mid - done >= CH) {
+            run_fused_graph(11, CH);
+            done += CH;
+        }
+        run_fused_graph(12, (int)(mid - done));
+    }
+
+    void fused_imag(long k) {
+        run_fused_graph(20, 0);
+        const int CH = kItChunk;
+        long done    = 0;
+        while (k - done >= CH) {
+            run_fused_graph(21, CH);
+            done += CH;
+        }
+        if (k - done > 0)
+            run_fused_graph(21, (int)(k - done));
+    }
+
     static constexpr int kItChunk = 64;
     static constexpr int kRtChunk = 32;
 
@@ -498,6 +798,12 @@ template <class R> class Solver final : public SolverBase {
     DevBuf<R> V, phi, vk;
     DevBuf<double> staging, norm_state, partial, epartial, eout;
     DevBuf<int> status, iter_zero, iter_base;
+    // fused pipeline (compile-time line lengths; complex64 only)
+    bool fused = false;
+    DevBuf<C> S2;
+    DevBuf<R> vk2;
+    DevBuf<double> zpartial;
+    DevBuf<unsigned> ticket;
     DevBuf<StepCoef> cur_coef, coef_dev;
     StepCoef host_coef{};
     StepCoef *coef_host   = nullptr;
@@ -1016,7 +1322,7 @@ int gpe_time_kernel(gpe_handle *h, int which, int reps, double *ms, double *byte
 const char *gpe_kernel_name(int which) {
     static const char *names[] = {"k_dip_z_fwd", "k_dip_y", "k_dip_x", "k_dip_y", "k_dip_z_inv",
                                   "k_kin_z", "k_kin_y", "k_kin_x", "k_kin_y", "k_kin_z",
-                                  "k_phase", "k_it_update"};
+                                  "k_phase", "k_it_update", "k2_x", "k2_y", "k2_z", "k2_y"};
     if (which < 0 || which >= GPE_K_COUNT)
         return "";
     return names[which];

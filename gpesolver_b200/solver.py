@@ -29,7 +29,8 @@ BECEnergies = namedtuple("BECEnergies", "e_kin e_pot e_int e_ext e_bmf e_total")
 PRECISIONS = {"c64": capi.GPE_PREC_C64, "c128": capi.GPE_PREC_C128}
 
 
-def make_gpe_params(p: PhysicalParameters, precision: str = "c64", device: int = 0) -> capi.gpe_params:
+def make_gpe_params(p: PhysicalParameters, precision: str = "c64", device: int = 0,
+                    schedule: str = "auto") -> capi.gpe_params:
     """Fill the C ABI's gpe_params from the PhysicalParameters fields."""
     g = capi.gpe_params()
     g.nx, g.ny, g.nz = p.nx, p.ny, p.nz
@@ -42,17 +43,19 @@ def make_gpe_params(p: PhysicalParameters, precision: str = "c64", device: int =
     g.iter_real = max(int(p.iter_real), 1)
     g.precision = PRECISIONS[precision]
     g.device = device
+    g.schedule = {"auto": capi.GPE_SCHED_AUTO, "split": capi.GPE_SCHED_SPLIT}[schedule]
     return g
 
 
 class B200GrossPitaevskiSolver:
-    def __init__(self, params: PhysicalParameters, precision: str = "c64", device: int = 0):
+    def __init__(self, params: PhysicalParameters, precision: str = "c64", device: int = 0,
+                 schedule: str = "auto"):
         # the solver owns its parameters (real_steps advances edd on this copy,
         # as calc_evolution advances the reference's singleton)
         self.params = dataclasses.replace(params)
         self.precision = precision
         self._L = capi.lib()
-        self._gp = make_gpe_params(params, precision, device)
+        self._gp = make_gpe_params(params, precision, device, schedule)
         h = ctypes.c_void_p()
         capi.check(self._L.gpe_create(ctypes.byref(self._gp), ctypes.byref(h)))
         self._h = h

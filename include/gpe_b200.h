@@ -65,7 +65,16 @@ typedef struct gpe_params {
     long iter_real;        /* ramp length (update_edd divides by it) */
     int precision;         /* GPE_PREC_* */
     int device;            /* CUDA device ordinal */
+    int schedule;          /* GPE_SCHED_*: kernel schedule of the fused iterations */
 } gpe_params;
+
+/* Kernel schedule of gpe_imag_steps / gpe_real_steps. */
+enum {
+    GPE_SCHED_AUTO  = 0, /* the four-kernel fused pipeline where the grid has compiled
+                            line lengths (nx, ny in {32,64,96,128,256}, nz in
+                            {8,16,24,32,64}, complex64), else the split schedule */
+    GPE_SCHED_SPLIT = 1  /* one kernel per FFT axis pass (any supported grid) */
+};
 
 typedef struct gpe_handle gpe_handle;
 
@@ -145,7 +154,10 @@ int gpe_launch_count(gpe_handle *h, long long *count);
 enum {
     GPE_K_DIP_Z_FWD = 0, GPE_K_DIP_Y_FWD, GPE_K_DIP_X, GPE_K_DIP_Y_INV, GPE_K_DIP_Z_INV,
     GPE_K_KIN_Z_FWD, GPE_K_KIN_Y_FWD, GPE_K_KIN_X, GPE_K_KIN_Y_INV, GPE_K_KIN_Z_INV,
-    GPE_K_PHASE, GPE_K_IT_UPDATE, GPE_K_COUNT
+    GPE_K_PHASE, GPE_K_IT_UPDATE,
+    /* the fused pipeline (real time): X pencils, Y inverse, Z rows, Y forward */
+    GPE_K_F_X, GPE_K_F_YINV, GPE_K_F_Z, GPE_K_F_YFWD,
+    GPE_K_COUNT
 };
 /* Launches kernel `which` `reps` times back to back on the handle's stream
  * between two CUDA events and reports the mean time per launch and the

@@ -48,6 +48,13 @@ def test_single_operations_match_golden(name, prec):
         np.testing.assert_allclose(e, g["op_energy"], rtol=ETOL[prec], atol=1e-30 + ETOL[prec] * abs(g["op_energy"][5]))
 
 
+def WELL_CONDITIONED(nx, ny, nz):
+    """Single-well, contact-dominated configuration (edd ramp 0.70 -> 0.80)."""
+    return O.default_config(nx=nx, ny=ny, nz=nz, init_strategy="GAUSS", pote_strategy="HARMONIC",
+                            dx=200.0, dy=200.0, dz=800.0, edd=None, edd_start=0.70, edd_stop=0.80,
+                            iter_real=500)
+
+
 def _rt_phase_max(name, g):
     """Largest nonlinear + external phase of one RT half step at the start of the
     RT phase of a fixture, from the FP64 golden data."""
@@ -115,17 +122,20 @@ def test_virtual_by_virtual_iterations_match_fused(prec):
     assert rel_l2(outs[0], outs[1]) < (1e-13 if prec == "c128" else 1e-6)
 
 
+@pytest.mark.parametrize("sched", ["split", "auto"])
 @pytest.mark.parametrize("prec", ["c64", "c128"])
 @pytest.mark.parametrize("k", [63, 64, 65, 130])
-def test_fused_chunks_equal_single_iterations(k, prec):
+def test_fused_chunks_equal_single_iterations(k, prec, sched):
     # The fused paths replay CUDA graphs of 64 (IT) / 32 (RT) iterations plus a
-    # remainder graph; k calls of one iteration must give the same bits.
-    cfg = O.default_config(nx=32, ny=32, nz=16, init_strategy="GAUSS", pote_strategy="HARMONIC",
-                           edd=None, edd_start=1.3, edd_stop=1.6, iter_real=200)
+    # remainder graph; k calls of one iteration must give the same bits with the
+    # split schedule.  The four-kernel pipeline (auto, complex64) merges the two
+    # potential half steps between consecutive iterations of one call, so there
+    # k single calls agree with one k-iteration call to rounding.
+    cfg = WELL_CONDITIONED(32, 32, 16)
     p = gparams(cfg)
     out = []
     for fused in (True, False):
-        with G.B200GrossPitaevskiSolver(p, precision=prec) as s:
+        with G.B200GrossPitaevskiSolver(p, precision=prec, schedule=sched) as s:
             s.load_pote(G.potential(p))
             s.load_buffer(G.initial_psi(p))
             if fused:
@@ -137,7 +147,10 @@ def test_fused_chunks_equal_single_iterations(k, prec):
                 for t in range(k):
                     s.real_steps(1, 7 + t)
             out.append(s.export_data())
-    np.testing.assert_array_equal(out[0], out[1])
+    if sched == "auto" and prec == "c64":
+        assert rel_l2(out[0], out[1]) < 1e-5
+    else:
+        np.testing.assert_array_equal(out[0], out[1])
 
 
 @pytest.mark.parametrize("k", [1, 2, 33])
@@ -240,3 +253,78 @@ def test_unsupported_grid_is_rejected():
     with pytest.raises(G.GpeError) as ei:
         G.B200GrossPitaevskiSolver(p)
     assert ei.value.code == 2
+
+
+FUSED_GRIDS = [(32, 32, 16), (64, 64, 16), (96, 96, 24), (128, 128, 32), (32, 64, 64)]
+
+
+@pytest.mark.parametrize("dims", FUSED_GRIDS)
+def test_fused_pipeline_matches_split_schedule(dims):
+    # the four-kernel fused pipeline (GPE_SCHED_AUTO on these grids) against the
+    # one-kernel-per-axis split schedule, both complex64, from the same state:
+    # IT then RT with an edd ramp.  The configuration is one the FP64 reference
+    # itself is stable on (a 1e-7 perturbation of psi_0 shrinks to ~1e-8 after
+    # these iterations); in the README's double well at these small boxes a
+    # 1e-7 perturbation grows to O(1) (the droplet picks a well), so no
+    # implementation with different rounding can be compared there.
+    cfg = WELL_CONDITIONED(*dims)
+    p = gparams(cfg)
+    V, psi0 = G.potential(p), G.initial_psi(p)
+    out, fi, en = [], [], []
+    for sched in ("auto", "split"):
+        with G.B200GrossPitaevskiSolver(p, precision="c64", schedule=sched) as s:
+            s.load_pote(V)
+            s.load_buffer(psi0)
+            s.imag_steps(70)
+            it_psi = s.export_data()
+            s.real_steps(45, 3)
+            out.append((it_psi, s.export_data()))
+            fi.append(s.export_fi3d())
+            en.append(s.calc_energy().e_total)
+    assert rel_l2(out[0][0], out[1][0]) < 2e-6
+    assert rel_l2(out[0][1], out[1][1]) < 2e-5
+    assert rel_l2(fi[0], fi[1]) < 2e-5
+    assert abs(en[0] - en[1]) < 1e-5 * abs(en[1])
+
+
+def test_fused_pipeline_matches_oracle_128():
+    cfg = O.default_config(nx=128, ny=128, nz=32, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
+                           pote_strategy="MEXICAN", fftw_n_threads=8)
+    p = gparams(cfg)
+    ref = O.OracleSolver(cfg)
+    ref.imag_steps(20)
+    with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
+        s.load_pote(G.potential(p))
+        s.load_buffer(G.initial_psi(p))
+        s.imag_steps(20)
+        assert rel_l2(s.export_data(), c128(ref.psi())) < 1e-5
+        assert rel_l2(s.export_fi3d(), ref.fi3d()) < 1e-5
+        ref.change_potential("MEXICAN_FREE")
+        s.load_pote(G.potential(p, "MEXICAN_FREE"))
+        ref.real_steps(20, 0)
+        s.real_steps(20, 0)
+        assert rel_l2(s.export_data(), c128(ref.psi())) < 2e-5
+        assert rel_l2(s.export_fi3d(), ref.fi3d()) < 2e-5
+    ref.close()
+
+
+@pytest.mark.parametrize("dims", [(64, 32, 8), (32, 32, 16), (128, 128, 32)])
+def test_fused_pipeline_short_runs_match_split(dims):
+    # a few iterations on the README's double well, before any instability can
+    # amplify rounding differences
+    nx, ny, nz = dims
+    cfg = O.default_config(nx=nx, ny=ny, nz=nz, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
+                           pote_strategy="MEXICAN")
+    p = gparams(cfg)
+    V, psi0 = G.potential(p), G.initial_psi(p)
+    for k in (1, 2, 3):
+        res = []
+        for sched in ("auto", "split"):
+            with G.B200GrossPitaevskiSolver(p, precision="c64", schedule=sched) as s:
+                s.load_pote(V)
+                s.load_buffer(psi0)
+                s.imag_steps(k)
+                s.real_steps(k, 0)
+                res.append((s.export_data(), s.export_fi3d()))
+        assert rel_l2(res[0][0], res[1][0]) < 1e-5
+        assert rel_l2(res[0][1], res[1][1]) < 1e-5
