@@ -117,7 +117,13 @@ __device__ __forceinline__ cplx<R> *ct_fft(cplx<R> *src, cplx<R> *dst, const cpl
 // back into the same buffer.  Needs one tile buffer instead of two (the
 // Stockham output order is kept).  ROUNDS = ceil(COUNT*L/RADIX / NT) butterflies
 // per thread are held at once.
-template <int SIGN, class R, int L, int RADIX, int NS, int COUNT, int TS, int NT>
+//   CMP  compensated twiddles (needed where the norm of psi must not drift;
+//        the dipolar potential's transforms run without)
+//   IH   first stage: only the lower half of each line is non-zero (zero-padded
+//        input); the upper half is neither read nor needs to be initialised
+//   OH   last stage: only the lower half of each line is kept (cropped output)
+template <int SIGN, class R, int L, int RADIX, int NS, int COUNT, int TS, int NT, bool CMP = true,
+          bool IH = false, bool OH = false>
 __device__ __forceinline__ void ct_stage_ip(cplx<R> *__restrict__ buf, const cplx<R> *__restrict__ tw,
                                             const cplx<R> *__restrict__ twlo, int tid) {
     using C                = cplx<R>;
@@ -137,11 +143,15 @@ __device__ __forceinline__ void ct_stage_ip(cplx<R> *__restrict__ buf, const cpl
         const C *s   = buf + b + j * TS;
 #pragma unroll
         for (int k = 0; k < RADIX; ++k) {
+            if (IH && NS == 1 && 2 * k >= RADIX) {
+                a[rd][k] = C{(R)0, (R)0};
+                continue;
+            }
             C v = s[k * NR * TS];
             if (NS > 1 && k > 0) {
                 const int t = jm * k * STEP;
                 const C w   = __ldg(&tw[t]);
-                if constexpr (sizeof(R) == 4)
+                if constexpr (sizeof(R) == 4 && CMP)
                     v = twmul<SIGN>(v, w, __ldg(&twlo[t]));
                 else
                     v = SIGN < 0 ? cmul(v, w) : cmulc(v, w);
@@ -158,24 +168,35 @@ __device__ __forceinline__ void ct_stage_ip(cplx<R> *__restrict__ buf, const cpl
         const int j  = it / COUNT;
         const int b  = it - j * COUNT;
         const int jm = j % NS;
-        DFT<RADIX, SIGN, R>::run(a[rd]);
+        DFT<RADIX, SIGN, R, CMP>::run(a[rd]);
         const int idxD = (j / NS) * NS * RADIX + jm;
         C *d           = buf + b + idxD * TS;
 #pragma unroll
         for (int q = 0; q < RADIX; ++q)
-            d[q * NS * TS] = a[rd][q];
+            if (!(OH && NS * RADIX == L && 2 * q >= RADIX))
+                d[q * NS * TS] = a[rd][q];
     }
     __syncthreads();
 }
 
-template <int SIGN, class R, int L, int COUNT, int TS, int NT, int S = 0, int NS = 1>
+template <int SIGN, class R, int L, int COUNT, int TS, int NT, bool CMP = true, bool IH = false,
+          bool OH = false, int S = 0, int NS = 1>
 __device__ __forceinline__ void ct_fft_ip(cplx<R> *buf, const cplx<R> *tw, const cplx<R> *twlo, int tid) {
     constexpr Radices RAD = radices_of(L);
     if constexpr (S < RAD.n) {
         constexpr int RADIX = RAD.r[S];
-        ct_stage_ip<SIGN, R, L, RADIX, NS, COUNT, TS, NT>(buf, tw, twlo, tid);
-        ct_fft_ip<SIGN, R, L, COUNT, TS, NT, S + 1, NS * RADIX>(buf, tw, twlo, tid);
+        // pruning needs an even radix on the pruned stage
+        constexpr bool ih = IH && S == 0 && RADIX % 2 == 0;
+        constexpr bool oh = OH && S == RAD.n - 1 && RADIX % 2 == 0;
+        ct_stage_ip<SIGN, R, L, RADIX, NS, COUNT, TS, NT, CMP, ih, oh>(buf, tw, twlo, tid);
+        ct_fft_ip<SIGN, R, L, COUNT, TS, NT, CMP, IH, OH, S + 1, NS * RADIX>(buf, tw, twlo, tid);
     }
+}
+
+// Whether ct_fft_ip prunes the first / last stage of a length-L transform.
+template <int L> constexpr bool ct_prunes_in() { return radices_of(L).r[0] % 2 == 0; }
+template <int L> constexpr bool ct_prunes_out() {
+    return radices_of(L).r[radices_of(L).n - 1] % 2 == 0;
 }
 
 // Number of stages (the result is in the first buffer when even).

@@ -93,9 +93,17 @@ __device__ __forceinline__ double cos16(int m) {
 }
 __device__ __forceinline__ double sin16(int m) { return cos16(m - 4); }
 
-template <int N, int SIGN, class R> struct DFT;
+// CMP: apply the radix-8/16/3/5/7 constants with the compensated multiply.
+template <int N, int SIGN, class R, bool CMP = true> struct DFT;
 
-template <int SIGN, class R> struct DFT<2, SIGN, R> {
+template <int SIGN, class C, class R, bool CMP> __device__ __forceinline__ C mul_wc(C a, double c, double s) {
+    if constexpr (CMP)
+        return mul_wk<SIGN, C, R>(a, c, s);
+    else
+        return mul_w<SIGN>(a, (R)c, (R)s);
+}
+
+template <int SIGN, class R, bool CMP> struct DFT<2, SIGN, R, CMP> {
     using C = cplx<R>;
     static __device__ __forceinline__ void run(C *a) {
         C t = a[0];
@@ -104,7 +112,7 @@ template <int SIGN, class R> struct DFT<2, SIGN, R> {
     }
 };
 
-template <int SIGN, class R> struct DFT<4, SIGN, R> {
+template <int SIGN, class R, bool CMP> struct DFT<4, SIGN, R, CMP> {
     using C = cplx<R>;
     static __device__ __forceinline__ void run(C *a) {
         C t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
@@ -118,7 +126,7 @@ template <int SIGN, class R> struct DFT<4, SIGN, R> {
 
 // N = N1 * N2 split in registers: x[N2 n1 + n2] -> X[k1 + N1 k2]
 //   y[n2][k1] = DFT_N1(x[N2 n1 + n2]) * W_N^{n2 k1};  X[k1 + N1 k2] = DFT_N2(y[.][k1])
-template <int N1, int N2, int SIGN, class R> struct DFTSplit {
+template <int N1, int N2, int SIGN, class R, bool CMP = true> struct DFTSplit {
     using C = cplx<R>;
     static __device__ __forceinline__ void run(C *a) {
         constexpr int N = N1 * N2;
@@ -128,7 +136,7 @@ template <int N1, int N2, int SIGN, class R> struct DFTSplit {
 #pragma unroll
             for (int n1 = 0; n1 < N1; ++n1)
                 y[n2][n1] = a[N2 * n1 + n2];
-            DFT<N1, SIGN, R>::run(y[n2]);
+            DFT<N1, SIGN, R, CMP>::run(y[n2]);
 #pragma unroll
             for (int k1 = 0; k1 < N1; ++k1) {
                 const int m = (n2 * k1 * (16 / N)) & 15;
@@ -137,7 +145,7 @@ template <int N1, int N2, int SIGN, class R> struct DFTSplit {
                 else if (m == 8)
                     y[n2][k1] = C{-y[n2][k1].x, -y[n2][k1].y};
                 else if (m != 0)
-                    y[n2][k1] = mul_wk<SIGN, C, R>(y[n2][k1], cos16(m), sin16(m));
+                    y[n2][k1] = mul_wc<SIGN, C, R, CMP>(y[n2][k1], cos16(m), sin16(m));
             }
         }
 #pragma unroll
@@ -146,7 +154,7 @@ template <int N1, int N2, int SIGN, class R> struct DFTSplit {
 #pragma unroll
             for (int n2 = 0; n2 < N2; ++n2)
                 z[n2] = y[n2][k1];
-            DFT<N2, SIGN, R>::run(z);
+            DFT<N2, SIGN, R, CMP>::run(z);
 #pragma unroll
             for (int k2 = 0; k2 < N2; ++k2)
                 a[k1 + N1 * k2] = z[k2];
@@ -154,11 +162,11 @@ template <int N1, int N2, int SIGN, class R> struct DFTSplit {
     }
 };
 
-template <int SIGN, class R> struct DFT<8, SIGN, R> {
-    static __device__ __forceinline__ void run(cplx<R> *a) { DFTSplit<4, 2, SIGN, R>::run(a); }
+template <int SIGN, class R, bool CMP> struct DFT<8, SIGN, R, CMP> {
+    static __device__ __forceinline__ void run(cplx<R> *a) { DFTSplit<4, 2, SIGN, R, CMP>::run(a); }
 };
-template <int SIGN, class R> struct DFT<16, SIGN, R> {
-    static __device__ __forceinline__ void run(cplx<R> *a) { DFTSplit<4, 4, SIGN, R>::run(a); }
+template <int SIGN, class R, bool CMP> struct DFT<16, SIGN, R, CMP> {
+    static __device__ __forceinline__ void run(cplx<R> *a) { DFTSplit<4, 4, SIGN, R, CMP>::run(a); }
 };
 
 // Odd prime radices: direct r-point sums with the constant table cos/sin(2 pi m / r).
@@ -211,7 +219,7 @@ template <> struct OddTab<7> {
     }
 };
 
-template <int P, int SIGN, class R> struct DFTOdd {
+template <int P, int SIGN, class R, bool CMP = true> struct DFTOdd {
     using C = cplx<R>;
     static __device__ __forceinline__ void run(C *a) {
         C out[P];
@@ -221,7 +229,7 @@ template <int P, int SIGN, class R> struct DFTOdd {
 #pragma unroll
             for (int k = 1; k < P; ++k) {
                 const int m = (k * q) % P;
-                acc         = cadd(acc, mul_wk<SIGN, C, R>(a[k], OddTab<P>::c(m), OddTab<P>::s(m)));
+                acc         = cadd(acc, mul_wc<SIGN, C, R, CMP>(a[k], OddTab<P>::c(m), OddTab<P>::s(m)));
             }
             out[q] = acc;
         }
@@ -230,14 +238,14 @@ template <int P, int SIGN, class R> struct DFTOdd {
             a[q] = out[q];
     }
 };
-template <int SIGN, class R> struct DFT<3, SIGN, R> {
-    static __device__ __forceinline__ void run(cplx<R> *a) { DFTOdd<3, SIGN, R>::run(a); }
+template <int SIGN, class R, bool CMP> struct DFT<3, SIGN, R, CMP> {
+    static __device__ __forceinline__ void run(cplx<R> *a) { DFTOdd<3, SIGN, R, CMP>::run(a); }
 };
-template <int SIGN, class R> struct DFT<5, SIGN, R> {
-    static __device__ __forceinline__ void run(cplx<R> *a) { DFTOdd<5, SIGN, R>::run(a); }
+template <int SIGN, class R, bool CMP> struct DFT<5, SIGN, R, CMP> {
+    static __device__ __forceinline__ void run(cplx<R> *a) { DFTOdd<5, SIGN, R, CMP>::run(a); }
 };
-template <int SIGN, class R> struct DFT<7, SIGN, R> {
-    static __device__ __forceinline__ void run(cplx<R> *a) { DFTOdd<7, SIGN, R>::run(a); }
+template <int SIGN, class R, bool CMP> struct DFT<7, SIGN, R, CMP> {
+    static __device__ __forceinline__ void run(cplx<R> *a) { DFTOdd<7, SIGN, R, CMP>::run(a); }
 };
 
 // Plan of one line transform of length L (host-built; passed by value).

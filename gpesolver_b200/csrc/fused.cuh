@@ -55,7 +55,7 @@ enum { ZM_RT_PRO = 0, ZM_RT_MID, ZM_RT_EPI, ZM_IT_PRO, ZM_IT_MID };
 // X pencils
 // ---------------------------------------------------------------------------
 template <class R, int NX, bool KIN>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 5)
     k2_x(cplx<R> *__restrict__ psi, cplx<R> *__restrict__ S, const R *__restrict__ vk,
          const cplx<R> *__restrict__ ex, const cplx<R> *__restrict__ ey, const cplx<R> *__restrict__ ez,
          R inv_hi, R inv_lo, const double *__restrict__ divisor, double dip_scale, int ny, int nz,
@@ -78,13 +78,17 @@ __global__ void __launch_bounds__(256, 4)
         ct_fft_ip<-1, R, NX, CK, CK, NT>(b0, (const C *)tk.tw, (const C *)tk.lo, tid);
         C *r1 = b0;
         {
-            // each thread keeps one column b for all its elements when CK | NT
-            for (int e = tid; e < CK * NX; e += NT) {
-                const int i = e / CK, b = e % CK;
+            // NT is a multiple of CK: each thread keeps one column b
+            static_assert(NT % CK == 0, "tile width must divide the block");
+            const int b = tid % CK;
+            if (b < cnt) {
                 const int c = c0 + b, j = c / nz, k = c - j * nz;
-                if (b < cnt) {
-                    const C w = combine_wm1(__ldg(&ex[i]), __ldg(&ey[j]), __ldg(&ez[k]));
-                    const C v = apply_wm1(r1[b + i * CK], w);
+                const C wyz = cadd(cadd(__ldg(&ey[j]), __ldg(&ez[k])), cmul(__ldg(&ey[j]), __ldg(&ez[k])));
+#pragma unroll 4
+                for (int i = tid / CK; i < NX; i += NT / CK) {
+                    const C wx = __ldg(&ex[i]);
+                    const C w  = cadd(cadd(wx, wyz), cmul(wx, wyz)); // (1+wx)(1+wyz) - 1
+                    const C v  = apply_wm1(r1[b + i * CK], w);
                     r1[b + i * CK] = C{fma(v.x, inv_hi, v.x * inv_lo), fma(v.y, inv_hi, v.y * inv_lo)};
                 }
             }
@@ -104,28 +108,35 @@ __global__ void __launch_bounds__(256, 4)
     const int cols   = 2 * ny * nz;
     const int c0     = ((int)blockIdx.x - (KIN ? nblk_kin : 0)) * CD;
     const int cnt    = min(CD, cols - c0);
+    // rows NX..L-1 are the zero padding: the pruned first stage does not read them
 #pragma unroll 4
     for (int e = tid; e < CD * NX; e += NT) {
         const int i = e / CD, b = e % CD;
-        b0[b + i * CD]        = b < cnt ? S[(size_t)i * cols + c0 + b] : C{(R)0, (R)0};
-        b0[b + (i + NX) * CD] = C{(R)0, (R)0};
+        b0[b + i * CD] = b < cnt ? S[(size_t)i * cols + c0 + b] : C{(R)0, (R)0};
     }
     __syncthreads();
-    ct_fft_ip<-1, R, L, CD, CD, NT>(b0, (const C *)td.tw, (const C *)td.lo, tid);
+    ct_fft_ip<-1, R, L, CD, CD, NT, false, true, false>(b0, (const C *)td.tw, (const C *)td.lo, tid);
     C *r1 = b0;
     // V_dd(k) * scale; scale = 1/(8N) (C2R normalisation) and, for imaginary
     // time, 1/xnorma (the spectrum was built from the unnormalised psi)
     const R scale = (R)(divisor ? dip_scale / divisor[0] : dip_scale);
-    for (int e = tid; e < CD * L; e += NT) {
-        const int t = e / CD, b = e % CD;
-        const int c = c0 + b, ky = c / nz, kz = c - ky * nz;
-        const int ix = t <= NX ? t : L - t;
-        const int iy = ky <= ny ? ky : 2 * ny - ky;
-        const R v    = (b < cnt) ? __ldg(&vk[((size_t)ix * (ny + 1) + iy) * nz + kz]) * scale : (R)0;
-        r1[b + t * CD] = cscale(r1[b + t * CD], v);
+    {
+        static_assert(NT % CD == 0, "tile width must divide the block");
+        const int b = tid % CD;
+        if (b < cnt) {
+            const int c = c0 + b, ky = c / nz, kz = c - ky * nz;
+            const int iy = ky <= ny ? ky : 2 * ny - ky;
+            const R *vcol = vk + (size_t)iy * nz + kz; // + ix * (ny+1) * nz
+            const size_t xs = (size_t)(ny + 1) * nz;
+#pragma unroll 4
+            for (int t = tid / CD; t < L; t += NT / CD) {
+                const int ix = t <= NX ? t : L - t;
+                r1[b + t * CD] = cscale(r1[b + t * CD], __ldg(&vcol[ix * xs]) * scale);
+            }
+        }
     }
     __syncthreads();
-    ct_fft_ip<+1, R, L, CD, CD, NT>(b0, (const C *)td.tw, (const C *)td.lo, tid);
+    ct_fft_ip<+1, R, L, CD, CD, NT, false, false, true>(b0, (const C *)td.tw, (const C *)td.lo, tid);
 #pragma unroll 4
     for (int e = tid; e < CD * NX; e += NT) {
         const int i = e / CD, b = e % CD;
@@ -171,11 +182,11 @@ __global__ void __launch_bounds__(256, 4)
     const int cnt    = min(CD, nz - k0);
     C *plane         = S + (size_t)i * L * nz;
     if (SIGN < 0) {
+        // rows NY..L-1 are the zero padding (not read by the pruned first stage)
 #pragma unroll 4
         for (int e = tid; e < CD * NY; e += NT) {
             const int j = e / CD, b = e % CD;
-            b0[b + j * CD]        = b < cnt ? plane[(size_t)j * nz + k0 + b] : C{(R)0, (R)0};
-            b0[b + (j + NY) * CD] = C{(R)0, (R)0};
+            b0[b + j * CD] = b < cnt ? plane[(size_t)j * nz + k0 + b] : C{(R)0, (R)0};
         }
     } else {
 #pragma unroll 4
@@ -185,7 +196,8 @@ __global__ void __launch_bounds__(256, 4)
         }
     }
     __syncthreads();
-    ct_fft_ip<SIGN, R, L, CD, CD, NT>(b0, (const C *)td.tw, (const C *)td.lo, tid);
+    ct_fft_ip<SIGN, R, L, CD, CD, NT, false, (SIGN < 0), (SIGN > 0)>(b0, (const C *)td.tw, (const C *)td.lo,
+                                                                     tid);
     const int rows_out = SIGN < 0 ? L : NY;
     for (int e = tid; e < CD * rows_out; e += NT) {
         const int j = e / CD, b = e % CD;
@@ -268,7 +280,7 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
             db0[p + m * TD] = z;
         }
         __syncthreads();
-        ct_fft_ip<+1, R, LD, NP, TD, NT>(db0, (const C *)td.tw, (const C *)td.lo, tid);
+        ct_fft_ip<+1, R, LD, NP, TD, NT, false, false, true>(db0, (const C *)td.tw, (const C *)td.lo, tid);
         const C *r = db0;
         R *phi_g = reinterpret_cast<R *>(a.phi);
         for (int e = tid; e < RW * NZ; e += NT) {
@@ -423,15 +435,13 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
 
     // ---- dipolar R2C of rho (row pairs) -> spectrum -------------------------
     if (HAS_FWD) {
-        for (int e = tid; e < NP * LD; e += NT) {
+        // rows NZ..LD-1 are the zero padding (not read by the pruned first stage)
+        for (int e = tid; e < NP * NZ; e += NT) {
             const int p = e % NP, m = e / NP;
-            C z         = C{(R)0, (R)0};
-            if (m < NZ)
-                z = C{phis[2 * p + m * TK], phis[2 * p + 1 + m * TK]};
-            db0[p + m * TD] = z;
+            db0[p + m * TD] = C{phis[2 * p + m * TK], phis[2 * p + 1 + m * TK]};
         }
         __syncthreads();
-        ct_fft_ip<-1, R, LD, NP, TD, NT>(db0, (const C *)td.tw, (const C *)td.lo, tid);
+        ct_fft_ip<-1, R, LD, NP, TD, NT, false, true, false>(db0, (const C *)td.tw, (const C *)td.lo, tid);
         const C *r = db0;
         for (int e = tid; e < RW * NZ; e += NT) {
             const int row = e / NZ, m = e % NZ + 1; // bins 1..NZ

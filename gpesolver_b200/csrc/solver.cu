@@ -170,6 +170,9 @@ template <class R> class Solver final : public SolverBase {
         GPE_CUDA(cudaSetDevice(p.device));
         GPE_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
         GPE_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+        GPE_CUDA(cudaStreamCreateWithFlags(&cap_stream2, cudaStreamNonBlocking));
+        GPE_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        GPE_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         cur = own_stream;
 
         plan_line(kz, nz, 16, 1);
@@ -222,6 +225,9 @@ template <class R> class Solver final : public SolverBase {
         if (coef_event)
             cudaEventDestroy(coef_event);
         cudaStreamSynchronize(cur);
+        cudaEventDestroy(ev_fork);
+        cudaEventDestroy(ev_join);
+        cudaStreamDestroy(cap_stream2);
         cudaStreamDestroy(cap_stream);
         cudaStreamDestroy(own_stream);
     }
@@ -622,7 +628,8 @@ template <class R> class Solver final : public SolverBase {
         }
     }
 
-    void f_x(cudaStream_t s, bool kin, const double *divisor) {
+    // part: 0 both, 1 kinetic only, 2 dipolar only
+    void f_x(cudaStream_t s, bool kin, const double *divisor, int part = 0) {
         if constexpr (std::is_same<R, float>::value) {
             const double dscale = 1.0 / (8.0 * (double)N);
 #define GPE_LX(NN)                                                                                 \
@@ -630,7 +637,11 @@ template <class R> class Solver final : public SolverBase {
         constexpr int CK = tile_lines<R, NN>(), CD = tile_lines<R, 2 * NN>();                     \
         const int nk = kin ? (ny * nz + CK - 1) / CK : 0;                                          \
         const int nd = (2 * ny * nz + CD - 1) / CD;                                                \
-        if (kin)                                                                                   \
+        if (kin && part == 1)                                                                      \
+            launch(k2_x<R, NN, true>, nk, 256, x_smem<NN>(true), s, psi.p, S2.p, (const R *)vk2.p,   \
+                   (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, divisor, dscale, \
+                   ny, nz, nk, twid(kx), twid(dx));                                                \
+        else if (kin && part == 0)                                                                 \
             launch(k2_x<R, NN, true>, nk + nd, 256, x_smem<NN>(true), s, psi.p, S2.p, (const R *)vk2.p, \
                    (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, divisor, dscale, \
                    ny, nz, nk, twid(kx), twid(dx));                                                \
@@ -644,14 +655,17 @@ template <class R> class Solver final : public SolverBase {
         }
     }
 
-    template <int SIGN> void f_y(cudaStream_t s, bool kin) {
+    template <int SIGN> void f_y(cudaStream_t s, bool kin, int part = 0) {
         if constexpr (std::is_same<R, float>::value) {
 #define GPE_LY(NN)                                                                                 \
     if (ny == NN) {                                                                                \
         constexpr int CK = y_ck<NN>(), CD = y_cd<NN>();                                            \
         const int nk = kin ? (nz + CK - 1) / CK : 0;                                               \
         const int nd = (nz + CD - 1) / CD;                                                         \
-        if (kin)                                                                                   \
+        if (kin && part == 1)                                                                      \
+            launch(k2_y<R, NN, SIGN, true>, dim3(nk, nx), 256, y_smem<NN>(true), s, psi.p, S2.p, nz, nk, \
+                   twid(ky), twid(dy));                                                            \
+        else if (kin && part == 0)                                                                 \
             launch(k2_y<R, NN, SIGN, true>, dim3(nk + nd, nx), 256, y_smem<NN>(true), s, psi.p, S2.p, \
                    nz, nk, twid(ky), twid(dy));                                                    \
         else                                                                                       \
@@ -704,16 +718,33 @@ template <class R> class Solver final : public SolverBase {
             f_z<ZM_RT_PRO>(s, psi.p, psi.p, coef_dev.p, 0);
             f_y<-1>(s, true);
         } else if (kind == 11 || kind == 12) {
-            for (int t = 0; t < count; ++t) {
-                f_x(s, true, nullptr);
-                f_y<+1>(s, true);
+            // the kinetic (s) and dipolar (s2) chains are independent until the Z
+            // kernel; they run as two branches of the graph
+            cudaStream_t s2 = cap_stream2;
+            for (int t = 0; t <= count; ++t) {
+                if (t == count && kind == 11)
+                    break;
+                GPE_CUDA(cudaEventRecord(ev_fork, s));
+                GPE_CUDA(cudaStreamWaitEvent(s2, ev_fork, 0));
+                f_x(s, true, nullptr, 1);
+                f_x(s2, false, nullptr);
+                f_y<+1>(s, true, 1);
+                f_y<+1>(s2, false);
+                GPE_CUDA(cudaEventRecord(ev_join, s2));
+                GPE_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
+                if (t == count) {
+                    f_z<ZM_RT_EPI>(s, psi.p, psi.p, coef_dev.p, count);
+                    break;
+                }
                 f_z<ZM_RT_MID>(s, psi.p, psi.p, coef_dev.p, t);
-                f_y<-1>(s, true);
+                GPE_CUDA(cudaEventRecord(ev_fork, s));
+                GPE_CUDA(cudaStreamWaitEvent(s2, ev_fork, 0));
+                f_y<-1>(s, true, 1);
+                f_y<-1>(s2, false);
+                GPE_CUDA(cudaEventRecord(ev_join, s2));
+                GPE_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
             }
             if (kind == 12) {
-                f_x(s, true, nullptr);
-                f_y<+1>(s, true);
-                f_z<ZM_RT_EPI>(s, psi.p, psi.p, coef_dev.p, count);
             } else {
                 launch(k_advance, 1, 1, 0, s, iter_base.p, count);
             }
@@ -810,7 +841,8 @@ template <class R> class Solver final : public SolverBase {
     size_t coef_cap       = 0;
     cudaEvent_t coef_event = nullptr;
     DevBuf<double> one_buf;
-    cudaStream_t own_stream = nullptr, cap_stream = nullptr, cur = nullptr;
+    cudaStream_t own_stream = nullptr, cap_stream = nullptr, cap_stream2 = nullptr, cur = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::map<std::tuple<int, int, const void *>, cudaGraphExec_t> graphs;
     std::map<std::tuple<int, int, const void *>, int> graph_nodes;
     int nblk_elem = 0;

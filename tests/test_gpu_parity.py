@@ -309,22 +309,26 @@ def test_fused_pipeline_matches_oracle_128():
 
 
 @pytest.mark.parametrize("dims", [(64, 32, 8), (32, 32, 16), (128, 128, 32)])
-def test_fused_pipeline_short_runs_match_split(dims):
-    # a few iterations on the README's double well, before any instability can
-    # amplify rounding differences
+def test_fused_pipeline_short_runs_match_oracle(dims):
+    # a few iterations on the README's double well: both complex64 schedules
+    # against the FP64 oracle (these small boxes hold a collapsing droplet, so
+    # the bound is the c64 one, 1e-4, rather than the well-conditioned 2e-5)
     nx, ny, nz = dims
     cfg = O.default_config(nx=nx, ny=ny, nz=nz, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
-                           pote_strategy="MEXICAN")
+                           pote_strategy="MEXICAN", fftw_n_threads=8)
     p = gparams(cfg)
     V, psi0 = G.potential(p), G.initial_psi(p)
-    for k in (1, 2, 3):
-        res = []
+    for k in (1, 3):
+        ref = O.OracleSolver(cfg)
+        ref.imag_steps(k)
+        ref.real_steps(k, 0)
+        want_psi, want_fi = c128(ref.psi()), ref.fi3d()
+        ref.close()
         for sched in ("auto", "split"):
             with G.B200GrossPitaevskiSolver(p, precision="c64", schedule=sched) as s:
                 s.load_pote(V)
                 s.load_buffer(psi0)
                 s.imag_steps(k)
                 s.real_steps(k, 0)
-                res.append((s.export_data(), s.export_fi3d()))
-        assert rel_l2(res[0][0], res[1][0]) < 1e-5
-        assert rel_l2(res[0][1], res[1][1]) < 1e-5
+                assert rel_l2(s.export_data(), want_psi) < 1e-4, sched
+                assert rel_l2(s.export_fi3d(), want_fi) < 1e-4, sched
