@@ -7,6 +7,11 @@ Two CPU FP64 implementations of GPESolver's solver hot path live under oracle/:
 * ``_ref/libgpe_ref.so``: the reference's own unmodified CPU sources compiled in
   place (oracle/Makefile) around a small harness (ref_harness.cpp).
 
+``_ref/libgpe_adapter.so`` (and ``_ref/libgpe_adapter_fused.so``) link the
+reference's own base class and driver with the B200 adapter
+(gpesolver_b200/adapter) instead of its CPU backend: the GPU tests use them to run
+the reference's control flow on the B200 backend.
+
 Both use the FP64 FFTW-API shim in oracle/fftw_shim because FFTW3 is not in this
 image.  Only tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU baseline
 import this module; the product path never does.
@@ -22,6 +27,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libgpe_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libgpe_ref.so")
+ADAPTER_SO = os.path.join(HERE, "_ref", "libgpe_adapter.so")
+ADAPTER_FUSED_SO = os.path.join(HERE, "_ref", "libgpe_adapter_fused.so")
+# calc_strategy of solve() (src/parameters/complex_param.hpp:14-20).
+STRATEGIES = {"IT": 0, "RT": 1, "FS": 2}
 
 # Potential ids in the reference's registration order (src/parameters/potentials.hpp:76-157).
 POTENTIALS = {
@@ -51,6 +60,8 @@ def build(ref: bool = True) -> None:
     targets = ["libgpe_oracle.so"]
     if ref and os.path.isdir(os.environ.get("GPE_REFERENCE_DIR", "/root/reference") + "/src"):
         targets.append("ref")
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "gpesolver_b200", "libgpe_b200.so")):
+            targets.append("adapter")
     subprocess.check_call(["make", "-s", "-C", HERE] + targets)
 
 
@@ -299,6 +310,10 @@ def rlib():
         L.gperef_update_edd.argtypes = [ctypes.c_long]
         L.gperef_change_potential.argtypes = [ctypes.c_char_p]
         L.gperef_op.argtypes = [ctypes.c_int]
+        L.gperef_solve.argtypes = [ctypes.c_int]
+        L.gperef_checkpoints.restype = ctypes.c_long
+        L.gperef_saved_energies.restype = ctypes.c_long
+        L.gperef_saved_energies.argtypes = [_dp, ctypes.c_long]
         _rlib = L
     return _rlib
 
@@ -306,6 +321,29 @@ def rlib():
 REF_OPS = {"calc_fi3d": 0, "imag_iter_linear_step": 1, "imag_iter_nonlinear_step": 2,
            "calc_norm": 3, "normalize": 4, "real_fft_potential_half_step": 5,
            "real_fft_kinetic_step": 6, "calc_energy": 7}
+
+
+def ref_config(cfg: dict, load_initial: bool = True) -> RefConfig:
+    """gperef_config from a gpe_params.json-style dict (default_config())."""
+    c = RefConfig()
+    c.nx, c.ny, c.nz = cfg["nx"], cfg["ny"], cfg["nz"]
+    c.dx_nm, c.dy_nm, c.dz_nm = cfg["dx"], cfg["dy"], cfg["dz"]
+    c.m_da, c.n_atoms = cfg["m"], cfg["n_atoms"]
+    c.omega_x_hz, c.omega_y_hz, c.omega_z_hz = cfg["omega_x"], cfg["omega_y"], cfg["omega_z"]
+    c.dd_nm = cfg["dd"]
+    if cfg.get("edd") is not None:
+        c.const_edd, c.edd = 1, cfg["edd"]
+    else:
+        c.const_edd, c.edd_start, c.edd_stop = 0, cfg["edd_start"], cfg["edd_stop"]
+    c.iter_imag, c.iter_real = cfg["iter_imag"], cfg["iter_real"]
+    c.init_strategy = INITS[cfg["init_strategy"]] if load_initial else 4
+    c.n_gauss_max = cfg.get("initial_maximas", 2)
+    c.bec_droplets_x = cfg.get("bec_droplets_x", 1)
+    c.bec_droplets_y = cfg.get("bec_droplets_y", 1)
+    c.bec_droplets_z = cfg.get("bec_droplets_z", 1)
+    c.fftw_n_threads = cfg.get("fftw_n_threads", 4)
+    c.pote_key = cfg["pote_strategy"].encode()
+    return c
 
 
 class RefSolver:
@@ -316,24 +354,7 @@ class RefSolver:
 
     def __init__(self, cfg: dict, load_initial: bool = True):
         L = rlib()
-        c = RefConfig()
-        c.nx, c.ny, c.nz = cfg["nx"], cfg["ny"], cfg["nz"]
-        c.dx_nm, c.dy_nm, c.dz_nm = cfg["dx"], cfg["dy"], cfg["dz"]
-        c.m_da, c.n_atoms = cfg["m"], cfg["n_atoms"]
-        c.omega_x_hz, c.omega_y_hz, c.omega_z_hz = cfg["omega_x"], cfg["omega_y"], cfg["omega_z"]
-        c.dd_nm = cfg["dd"]
-        if cfg.get("edd") is not None:
-            c.const_edd, c.edd = 1, cfg["edd"]
-        else:
-            c.const_edd, c.edd_start, c.edd_stop = 0, cfg["edd_start"], cfg["edd_stop"]
-        c.iter_imag, c.iter_real = cfg["iter_imag"], cfg["iter_real"]
-        c.init_strategy = INITS[cfg["init_strategy"]] if load_initial else 4
-        c.n_gauss_max = cfg.get("initial_maximas", 2)
-        c.bec_droplets_x = cfg.get("bec_droplets_x", 1)
-        c.bec_droplets_y = cfg.get("bec_droplets_y", 1)
-        c.bec_droplets_z = cfg.get("bec_droplets_z", 1)
-        c.fftw_n_threads = cfg.get("fftw_n_threads", 4)
-        c.pote_key = cfg["pote_strategy"].encode()
+        c = ref_config(cfg, load_initial)
         rc = L.gperef_create(ctypes.byref(c))
         if rc != 0:
             raise RuntimeError(L.gperef_last_error().decode())
@@ -394,3 +415,91 @@ class RefSolver:
         out = np.zeros(6)
         rlib().gperef_energy(_ptr(out))
         return out
+
+    def solve(self, strategy: str):
+        """AbstractGrossPitaevskiSolver::solve with calc_strategy IT / RT / FS."""
+        rc = rlib().gperef_solve(STRATEGIES[strategy])
+        if rc != 0:
+            raise RuntimeError(rlib().gperef_last_error().decode())
+
+    def checkpoints(self) -> int:
+        return rlib().gperef_checkpoints()
+
+    def saved_energies(self) -> np.ndarray:
+        return _saved_energies(rlib().gperef_saved_energies)
+
+
+def _saved_energies(fn) -> np.ndarray:
+    n = fn(None, 0)
+    out = np.zeros((max(n, 0), 6))
+    if n > 0:
+        fn(_ptr(out), n)
+    return out
+
+
+_alibs: dict = {}
+
+
+def alib(fused: bool = False):
+    path = ADAPTER_FUSED_SO if fused else ADAPTER_SO
+    if path not in _alibs:
+        L = ctypes.CDLL(path)
+        L.gpeadp_create.argtypes = [ctypes.POINTER(RefConfig), ctypes.c_int]
+        L.gpeadp_last_error.restype = ctypes.c_char_p
+        L.gpeadp_imag_steps.argtypes = [ctypes.c_long]
+        L.gpeadp_real_steps.argtypes = [ctypes.c_long, ctypes.c_long]
+        L.gpeadp_solve.argtypes = [ctypes.c_int]
+        L.gpeadp_export_psi.argtypes = [_dp]
+        L.gpeadp_energy.argtypes = [_dp]
+        L.gpeadp_checkpoints.restype = ctypes.c_long
+        L.gpeadp_saved_energies.restype = ctypes.c_long
+        L.gpeadp_saved_energies.argtypes = [_dp, ctypes.c_long]
+        _alibs[path] = L
+    return _alibs[path]
+
+
+class AdapterSolver:
+    """The reference's own AbstractGrossPitaevskiSolver code driving the B200
+    backend through gpesolver_b200/adapter (B200GrossPitaevskiSolver).
+
+    ``fused`` selects the build with GPE_B200_FUSED_LOOPS (calc_initial_state /
+    calc_evolution run as fused device calls).  Needs a GPU."""
+
+    def __init__(self, cfg: dict, precision: int = 0, fused: bool = False):
+        self.L = alib(fused)
+        rc = self.L.gpeadp_create(ctypes.byref(ref_config(cfg)), precision)
+        if rc != 0:
+            raise RuntimeError(self.L.gpeadp_last_error().decode())
+        self.n = cfg["nx"] * cfg["ny"] * cfg["nz"]
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.L.gpeadp_last_error().decode())
+
+    def close(self):
+        self.L.gpeadp_destroy()
+
+    def imag_steps(self, k: int):
+        self._check(self.L.gpeadp_imag_steps(k))
+
+    def real_steps(self, k: int, first_iter: int = 0):
+        self._check(self.L.gpeadp_real_steps(k, first_iter))
+
+    def solve(self, strategy: str):
+        self._check(self.L.gpeadp_solve(STRATEGIES[strategy]))
+
+    def psi(self) -> np.ndarray:
+        out = np.zeros(2 * self.n)
+        self._check(self.L.gpeadp_export_psi(_ptr(out)))
+        return out
+
+    def energy(self) -> np.ndarray:
+        out = np.zeros(6)
+        self._check(self.L.gpeadp_energy(_ptr(out)))
+        return out
+
+    def checkpoints(self) -> int:
+        return self.L.gpeadp_checkpoints()
+
+    def saved_energies(self) -> np.ndarray:
+        return _saved_energies(self.L.gpeadp_saved_energies)

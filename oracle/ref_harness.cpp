@@ -20,33 +20,14 @@
 #include "parameters/parameters.hpp"
 #include "solver/cpu_solver/cpu_solver.hpp"
 #include "solver/fft_solvers/cpu/fftw_abstract_cpu_solver.hpp"
+#include "ref_config.hpp"
 #include "units.hpp"
 
 #include <cstring>
 #include <memory>
 #include <stdexcept>
 #include <string>
-
-extern "C" {
-// Mirror of the gpe_params.json fields the reference loads
-// (src/filemanager/file_manager.cpp:436-541), in the file's units (nm, Da, Hz).
-struct gperef_config {
-    int nx, ny, nz;
-    double dx_nm, dy_nm, dz_nm;
-    double m_da;
-    double n_atoms;
-    double omega_x_hz, omega_y_hz, omega_z_hz;
-    double dd_nm;
-    int const_edd;
-    double edd, edd_start, edd_stop;
-    long iter_imag, iter_real;
-    int init_strategy; // 0 COS, 1 GAUSS, 2 MULTIPLE_GAUSS, 3 SETUP_GAUSS, 4 none (load later)
-    int n_gauss_max;
-    int bec_droplets_x, bec_droplets_y, bec_droplets_z;
-    int fftw_n_threads;
-    char pote_key[32];
-};
-}
+#include <vector>
 
 namespace {
 
@@ -65,9 +46,11 @@ public:
     void request_load_from_text(wavefunction_t &) override {}
     void request_free_potential() override { initializer->change_potential("MEXICAN_FREE"); }
     void save_data(const wavefunction_t &) override {}
-    void save_checkpoint(const wavefunction_t &) override {}
+    void save_checkpoint(const wavefunction_t &) override { ++checkpoints; }
     void save_initial_state(const wavefunction_t &) override {}
-    void save_energies(const energies_container_t &) override {}
+    void save_energies(const energies_container_t &e) override { energies = e; }
+    std::vector<BECEnergies> energies;
+    long checkpoints = 0;
 };
 
 // Exposes the protected step functions of the reference's base class and the
@@ -134,49 +117,7 @@ const char *gperef_last_error(void) { return g_err.c_str(); }
 int gperef_create(const gperef_config *c) {
     try {
         g_state.reset();
-        PhysicalParameters *p = PhysicalParameters::getInstance();
-        // Same conversions as FileManager::load_box / load_simulation / load_potential.
-        p->dx = UnitConverter::len_nm_to_au(c->dx_nm);
-        p->dy = UnitConverter::len_nm_to_au(c->dy_nm);
-        p->dz = UnitConverter::len_nm_to_au(c->dz_nm);
-        p->nx = c->nx;
-        p->ny = c->ny;
-        p->nz = c->nz;
-        p->iter_imag = (size_t)c->iter_imag;
-        p->iter_real = (size_t)c->iter_real;
-        p->n_atoms   = c->n_atoms;
-        p->m         = UnitConverter::mass_Da_to_au(c->m_da);
-        p->const_edd = c->const_edd != 0;
-        if (p->const_edd) {
-            p->edd = c->edd;
-        } else {
-            p->edd_start = c->edd_start;
-            p->edd_stop  = c->edd_stop;
-            // The reference leaves edd uninitialised when only a ramp is given
-            // (src/parameters/parameters.hpp:120); the harness defines it as edd_start.
-            p->edd = c->edd_start;
-        }
-        p->fftw_n_threads = c->fftw_n_threads > 0 ? c->fftw_n_threads : 4;
-        p->pote_key       = std::string(c->pote_key);
-        p->dd             = UnitConverter::len_nm_to_au(c->dd_nm);
-        p->omega_x        = UnitConverter::freq_Hz_to_au(c->omega_x_hz);
-        p->omega_y        = UnitConverter::freq_Hz_to_au(c->omega_y_hz);
-        p->omega_z        = UnitConverter::freq_Hz_to_au(c->omega_z_hz);
-        p->n_gauss_max    = c->n_gauss_max;
-        p->bec_droplets_x = c->bec_droplets_x;
-        p->bec_droplets_y = c->bec_droplets_y;
-        p->bec_droplets_z = c->bec_droplets_z;
-        switch (c->init_strategy) {
-        case 0: p->init_strategy.type = InitializationOption::Type::COS; break;
-        case 1: p->init_strategy.type = InitializationOption::Type::GAUSS; break;
-        case 2: p->init_strategy.type = InitializationOption::Type::MULTIPLE_GAUSS; break;
-        case 3: p->init_strategy.type = InitializationOption::Type::SETUP_GAUSS; break;
-        default: break;
-        }
-
-        // SimulationManager::on_params_loaded (src/manager/sim_manager.cpp:50-58).
-        p->init_parameters();
-        SimulationContext::getInstance()->initialize();
+        gperef_apply_config(c);
         auto st                 = std::make_unique<State>();
         st->solver              = std::make_unique<HarnessSolver>(&st->mediator);
         st->initializer         = std::make_unique<DataInitializer>(&st->mediator);
@@ -259,6 +200,36 @@ int gperef_real_steps(long k, long first_iter) {
         g_state->solver->real_time_iter();
     }
     return 0;
+}
+
+// AbstractGrossPitaevskiSolver::solve (src/solver/solver.cpp:25-46) with the
+// given strategy: 0 IT, 1 RT, 2 FULL.
+int gperef_solve(int strategy) {
+    if (!g_state) return 1;
+    try {
+        PhysicalParameters *p = PhysicalParameters::getInstance();
+        p->calc_strategy.type = strategy == 0   ? CalcStrategy::Type::IMAGINARY_TIME
+                                : strategy == 1 ? CalcStrategy::Type::REAL_TIME
+                                                : CalcStrategy::Type::FULL;
+        g_state->solver->solve();
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// What solve() handed to save_checkpoint / save_energies.
+long gperef_checkpoints(void) { return g_state ? g_state->mediator.checkpoints : -1; }
+
+long gperef_saved_energies(double *out, long max_rows) {
+    if (!g_state) return -1;
+    const auto &v = g_state->mediator.energies;
+    const long n  = (long)v.size();
+    for (long r = 0; r < n && r < max_rows; ++r) {
+        const double row[6] = {v[r].e_kin, v[r].e_pot, v[r].e_int, v[r].e_ext, v[r].e_bmf, v[r].e_total};
+        std::memcpy(out + 6 * r, row, sizeof(row));
+    }
+    return n;
 }
 
 // Individual virtuals, for per-operation parity checks.

@@ -54,3 +54,10 @@ def rel_l2(a, b) -> float:
 
 def c128(flat: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(flat).view(np.complex128)
+
+
+def WELL_CONDITIONED(nx, ny, nz):
+    """Single-well, contact-dominated configuration (edd ramp 0.70 -> 0.80)."""
+    return O.default_config(nx=nx, ny=ny, nz=nz, init_strategy="GAUSS", pote_strategy="HARMONIC",
+                            dx=200.0, dy=200.0, dz=800.0, edd=None, edd_start=0.70, edd_stop=0.80,
+                            iter_real=500)

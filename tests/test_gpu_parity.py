@@ -13,7 +13,7 @@ import pytest
 import gpesolver_b200 as G
 from oracle import oracle as O
 
-from .helpers import c128, golden, golden_cases, gparams, rel_l2
+from .helpers import WELL_CONDITIONED, c128, golden, golden_cases, gparams, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -46,13 +46,6 @@ def test_single_operations_match_golden(name, prec):
         assert rel_l2(s.export_data(), c128(g["op_kinetic"])) < TOL[prec]
         e = np.array(s.calc_energy())
         np.testing.assert_allclose(e, g["op_energy"], rtol=ETOL[prec], atol=1e-30 + ETOL[prec] * abs(g["op_energy"][5]))
-
-
-def WELL_CONDITIONED(nx, ny, nz):
-    """Single-well, contact-dominated configuration (edd ramp 0.70 -> 0.80)."""
-    return O.default_config(nx=nx, ny=ny, nz=nz, init_strategy="GAUSS", pote_strategy="HARMONIC",
-                            dx=200.0, dy=200.0, dz=800.0, edd=None, edd_start=0.70, edd_stop=0.80,
-                            iter_real=500)
 
 
 def _rt_phase_max(name, g):
