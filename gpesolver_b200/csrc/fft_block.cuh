@@ -126,7 +126,10 @@ template <int SIGN, class R, bool CMP> struct DFT<4, SIGN, R, CMP> {
 
 // N = N1 * N2 split in registers: x[N2 n1 + n2] -> X[k1 + N1 k2]
 //   y[n2][k1] = DFT_N1(x[N2 n1 + n2]) * W_N^{n2 k1};  X[k1 + N1 k2] = DFT_N2(y[.][k1])
-template <int N1, int N2, int SIGN, class R, bool CMP = true> struct DFTSplit {
+//   Z1 < N1: only x[N2 n1 + n2] with n1 < Z1 are non-zero (the first N Z1 / N1
+//   inputs); the zeros are neither read nor added (DFTZ below).
+template <int N, int SIGN, class R, bool CMP, int ZIN> struct DFTZ;
+template <int N1, int N2, int SIGN, class R, bool CMP = true, int Z1 = N1> struct DFTSplit {
     using C = cplx<R>;
     static __device__ __forceinline__ void run(C *a) {
         constexpr int N = N1 * N2;
@@ -135,8 +138,8 @@ template <int N1, int N2, int SIGN, class R, bool CMP = true> struct DFTSplit {
         for (int n2 = 0; n2 < N2; ++n2) {
 #pragma unroll
             for (int n1 = 0; n1 < N1; ++n1)
-                y[n2][n1] = a[N2 * n1 + n2];
-            DFT<N1, SIGN, R, CMP>::run(y[n2]);
+                y[n2][n1] = n1 < Z1 ? a[N2 * n1 + n2] : C{(R)0, (R)0};
+            DFTZ<N1, SIGN, R, CMP, Z1>::run(y[n2]);
 #pragma unroll
             for (int k1 = 0; k1 < N1; ++k1) {
                 const int m = (n2 * k1 * (16 / N)) & 15;
@@ -167,6 +170,32 @@ template <int SIGN, class R, bool CMP> struct DFT<8, SIGN, R, CMP> {
 };
 template <int SIGN, class R, bool CMP> struct DFT<16, SIGN, R, CMP> {
     static __device__ __forceinline__ void run(cplx<R> *a) { DFTSplit<4, 4, SIGN, R, CMP>::run(a); }
+};
+
+// DFT of N points of which only the first ZIN are non-zero (ZIN = N or N / 2):
+// the pruned first stage of a zero-padded transform.  a[ZIN..N-1] are not read.
+template <int N, int SIGN, class R, bool CMP, int ZIN> struct DFTZ {
+    static_assert(ZIN == N, "pruned DFT: N in {2, 4, 8, 16} with ZIN = N / 2");
+    static __device__ __forceinline__ void run(cplx<R> *a) { DFT<N, SIGN, R, CMP>::run(a); }
+};
+template <int SIGN, class R, bool CMP> struct DFTZ<2, SIGN, R, CMP, 1> {
+    static __device__ __forceinline__ void run(cplx<R> *a) { a[1] = a[0]; }
+};
+template <int SIGN, class R, bool CMP> struct DFTZ<4, SIGN, R, CMP, 2> {
+    using C = cplx<R>;
+    static __device__ __forceinline__ void run(C *a) {
+        const C x0 = a[0], x1 = a[1], t3 = mul_si<SIGN>(a[1]);
+        a[0] = cadd(x0, x1);
+        a[2] = csub(x0, x1);
+        a[1] = cadd(x0, t3);
+        a[3] = csub(x0, t3);
+    }
+};
+template <int SIGN, class R, bool CMP> struct DFTZ<8, SIGN, R, CMP, 4> {
+    static __device__ __forceinline__ void run(cplx<R> *a) { DFTSplit<4, 2, SIGN, R, CMP, 2>::run(a); }
+};
+template <int SIGN, class R, bool CMP> struct DFTZ<16, SIGN, R, CMP, 8> {
+    static __device__ __forceinline__ void run(cplx<R> *a) { DFTSplit<4, 4, SIGN, R, CMP, 2>::run(a); }
 };
 
 // Odd prime radices: direct r-point sums with the constant table cos/sin(2 pi m / r).

@@ -25,6 +25,7 @@
 
 #include "ct_fft.cuh"
 #include "kernels.cuh"
+#include "rfft.cuh"
 
 namespace gpe {
 
@@ -54,157 +55,171 @@ enum { ZM_RT_PRO = 0, ZM_RT_MID, ZM_RT_EPI, ZM_IT_PRO, ZM_IT_MID };
 // ---------------------------------------------------------------------------
 // X pencils
 // ---------------------------------------------------------------------------
-template <class R, int NX, bool KIN>
-__global__ void __launch_bounds__(256, 5)
-    k2_x(cplx<R> *__restrict__ psi, cplx<R> *__restrict__ S, const R *__restrict__ vk,
-         const cplx<R> *__restrict__ ex, const cplx<R> *__restrict__ ey, const cplx<R> *__restrict__ ez,
-         R inv_hi, R inv_lo, const double *__restrict__ divisor, double dip_scale, int ny, int nz,
-         int nblk_kin, Twid tk, Twid td) {
-    using C          = cplx<R>;
-    constexpr int NT = 256;
-    const int tid    = threadIdx.x;
-    C *b0            = reinterpret_cast<C *>(g_smem);
-    if (KIN && (int)blockIdx.x < nblk_kin) {
-        constexpr int CK = tile_lines<R, NX>();
-        const int cols   = ny * nz;
-        const int c0     = blockIdx.x * CK;
-        const int cnt    = min(CK, cols - c0);
-#pragma unroll 4
-        for (int e = tid; e < CK * NX; e += NT) {
-            const int i = e / CK, b = e % CK;
-            b0[b + i * CK] = b < cnt ? psi[(size_t)i * cols + c0 + b] : C{(R)0, (R)0};
-        }
-        __syncthreads();
-        ct_fft_ip<-1, R, NX, CK, CK, NT>(b0, (const C *)tk.tw, (const C *)tk.lo, tid);
-        C *r1 = b0;
-        {
-            // NT is a multiple of CK: each thread keeps one column b
-            static_assert(NT % CK == 0, "tile width must divide the block");
-            const int b = tid % CK;
-            if (b < cnt) {
-                const int c = c0 + b, j = c / nz, k = c - j * nz;
-                const C wyz = cadd(cadd(__ldg(&ey[j]), __ldg(&ez[k])), cmul(__ldg(&ey[j]), __ldg(&ez[k])));
-#pragma unroll 4
-                for (int i = tid / CK; i < NX; i += NT / CK) {
-                    const C wx = __ldg(&ex[i]);
-                    const C w  = cadd(cadd(wx, wyz), cmul(wx, wyz)); // (1+wx)(1+wyz) - 1
-                    const C v  = apply_wm1(r1[b + i * CK], w);
-                    r1[b + i * CK] = C{fma(v.x, inv_hi, v.x * inv_lo), fma(v.y, inv_hi, v.y * inv_lo)};
-                }
-            }
-        }
-        __syncthreads();
-        ct_fft_ip<+1, R, NX, CK, CK, NT>(b0, (const C *)tk.tw, (const C *)tk.lo, tid);
-#pragma unroll 4
-        for (int e = tid; e < CK * NX; e += NT) {
-            const int i = e / CK, b = e % CK;
-            if (b < cnt)
-                psi[(size_t)i * cols + c0 + b] = b0[b + i * CK];
-        }
-        return;
-    }
-    constexpr int L  = 2 * NX;
-    constexpr int CD = tile_lines<R, L>();
-    const int cols   = 2 * ny * nz;
-    const int c0     = ((int)blockIdx.x - (KIN ? nblk_kin : 0)) * CD;
-    const int cnt    = min(CD, cols - c0);
-    // rows NX..L-1 are the zero padding: the pruned first stage does not read them
-#pragma unroll 4
-    for (int e = tid; e < CD * NX; e += NT) {
-        const int i = e / CD, b = e % CD;
-        b0[b + i * CD] = b < cnt ? S[(size_t)i * cols + c0 + b] : C{(R)0, (R)0};
-    }
-    __syncthreads();
-    ct_fft_ip<-1, R, L, CD, CD, NT, false, true, false>(b0, (const C *)td.tw, (const C *)td.lo, tid);
-    C *r1 = b0;
-    // V_dd(k) * scale; scale = 1/(8N) (C2R normalisation) and, for imaginary
-    // time, 1/xnorma (the spectrum was built from the unnormalised psi)
-    const R scale = (R)(divisor ? dip_scale / divisor[0] : dip_scale);
+// Lines per CTA of the x and y passes: 16 (an 8-byte complex row segment of
+// 128 bytes per line, coalesced), 8 for the 512-point dipolar lines.
+template <int L> constexpr int xy_count() { return L >= 512 ? 8 : 16; }
+
+// Kinetic x pencils: psi(x, ky, kz) -> FFT_x -> exp(i(-dt/2m)k^2) / N -> iFFT_x.
+// The forward transform ends and the inverse one starts in registers, with the
+// kinetic phase applied in between.
+template <class R, int NX, int CNT, int NT>
+__global__ void __launch_bounds__(NT)
+    k3_x_kin(cplx<R> *__restrict__ psi, const cplx<R> *__restrict__ ex, const cplx<R> *__restrict__ ey,
+             const cplx<R> *__restrict__ ez, R inv_hi, R inv_lo, int ny, int nz, Twid tk) {
+    using C  = cplx<R>;
+    using Fw = LinePass<-1, R, NX, CNT, CNT, NT, true, false>;
+    using Iv = LinePass<+1, R, NX, CNT, CNT, NT, true, true>;
+    static_assert(Fw::RL == Iv::R0 && Fw::ROUNDSL == Iv::ROUNDS0 && Fw::ITEMSL == Iv::ITEMS0,
+                  "paired transforms share the register layout");
+    const int tid  = threadIdx.x;
+    C *buf         = reinterpret_cast<C *>(g_smem);
+    const C *tw    = (const C *)tk.tw, *tl = (const C *)tk.lo;
+    const int cols = ny * nz;
+    const int c0   = blockIdx.x * CNT;
+    const int cnt  = min(CNT, cols - c0);
+    C a[Fw::ROUNDSL][Fw::RL];
+    Fw::run_to_regs(
+        buf, [&](int b, int t) { return b < cnt ? psi[(size_t)t * cols + c0 + b] : C{(R)0, (R)0}; }, a, tw, tl,
+        tid);
     {
-        static_assert(NT % CD == 0, "tile width must divide the block");
-        const int b = tid % CD;
+        const int b = Fw::line_of(tid);
+        C wyz       = C{(R)0, (R)0};
         if (b < cnt) {
-            const int c = c0 + b, ky = c / nz, kz = c - ky * nz;
-            const int iy = ky <= ny ? ky : 2 * ny - ky;
-            const R *vcol = vk + (size_t)iy * nz + kz; // + ix * (ny+1) * nz
-            const size_t xs = (size_t)(ny + 1) * nz;
-#pragma unroll 4
-            for (int t = tid / CD; t < L; t += NT / CD) {
-                const int ix = t <= NX ? t : L - t;
-                r1[b + t * CD] = cscale(r1[b + t * CD], __ldg(&vcol[ix * xs]) * scale);
+            const int c = c0 + b, j = c / nz, k = c - j * nz;
+            const C wy = __ldg(&ey[j]), wz = __ldg(&ez[k]);
+            wyz        = cadd(cadd(wy, wz), cmul(wy, wz)); // (1+wy)(1+wz) - 1
+        }
+#pragma unroll
+        for (int rd = 0; rd < Fw::ROUNDSL; ++rd) {
+            if (!Fw::template valid<Fw::ITEMSL>(rd * NT + tid))
+                break;
+#pragma unroll
+            for (int q = 0; q < Fw::RL; ++q) {
+                const C wx = __ldg(&ex[Fw::last_index(tid, rd, q)]);
+                const C w  = cadd(cadd(wx, wyz), cmul(wx, wyz)); // (1+wx)(1+wyz) - 1
+                const C v  = apply_wm1(a[rd][q], w);
+                a[rd][q]   = C{fma(v.x, inv_hi, v.x * inv_lo), fma(v.y, inv_hi, v.y * inv_lo)};
             }
         }
     }
     __syncthreads();
-    ct_fft_ip<+1, R, L, CD, CD, NT, false, false, true>(b0, (const C *)td.tw, (const C *)td.lo, tid);
-#pragma unroll 4
-    for (int e = tid; e < CD * NX; e += NT) {
-        const int i = e / CD, b = e % CD;
-        if (b < cnt)
-            S[(size_t)i * cols + c0 + b] = b0[b + i * CD];
+    Iv::run_from_regs(
+        buf, a,
+        [&](int b, int t, C v) {
+            if (b < cnt)
+                psi[(size_t)t * cols + c0 + b] = v;
+        },
+        tw, tl, tid);
+}
+
+// Dipolar x pencils: S(x, ky, kz) -> FFT_2nx (upper half zero) -> V_dd(k) * scale
+// -> iFFT_2nx, lower half kept.  scale = 1/(8N) (C2R normalisation) and, in
+// imaginary time, 1/xnorma (the spectrum was built from the unnormalised psi).
+template <class R, int NX, int CNT, int NT>
+__global__ void __launch_bounds__(NT)
+    k3_x_dip(cplx<R> *__restrict__ S, const R *__restrict__ vk, const double *__restrict__ divisor,
+             double dip_scale, int ny, int nz, Twid td) {
+    using C          = cplx<R>;
+    constexpr int L  = 2 * NX;
+    using Fw         = LinePass<-1, R, L, CNT, CNT, NT, false, false, true, false>;
+    using Iv         = LinePass<+1, R, L, CNT, CNT, NT, false, true, false, true>;
+    static_assert(Fw::RL == Iv::R0 && Fw::ROUNDSL == Iv::ROUNDS0 && Fw::ITEMSL == Iv::ITEMS0,
+                  "paired transforms share the register layout");
+    const int tid  = threadIdx.x;
+    C *buf         = reinterpret_cast<C *>(g_smem);
+    const C *tw    = (const C *)td.tw, *tl = (const C *)td.lo;
+    const int cols = 2 * ny * nz;
+    const int c0   = blockIdx.x * CNT;
+    const int cnt  = min(CNT, cols - c0);
+    C a[Fw::ROUNDSL][Fw::RL];
+    Fw::run_to_regs(
+        buf, [&](int b, int t) { return b < cnt ? S[(size_t)t * cols + c0 + b] : C{(R)0, (R)0}; }, a, tw, tl,
+        tid);
+    {
+        const R scale = (R)(divisor ? dip_scale / divisor[0] : dip_scale);
+        const int b   = Fw::line_of(tid);
+        const int c   = min(c0 + b, cols - 1);
+        const int ky = c / nz, kz = c - ky * nz;
+        const int iy      = ky <= ny ? ky : 2 * ny - ky;
+        const R *vcol     = vk + (size_t)iy * nz + kz; // + ix * (ny+1) * nz
+        const size_t xs   = (size_t)(ny + 1) * nz;
+#pragma unroll
+        for (int rd = 0; rd < Fw::ROUNDSL; ++rd) {
+            if (!Fw::template valid<Fw::ITEMSL>(rd * NT + tid))
+                break;
+#pragma unroll
+            for (int q = 0; q < Fw::RL; ++q) {
+                const int t  = Fw::last_index(tid, rd, q);
+                const int ix = t <= NX ? t : L - t;
+                a[rd][q]     = cscale(a[rd][q], __ldg(&vcol[ix * xs]) * scale);
+            }
+        }
     }
+    __syncthreads();
+    Iv::run_from_regs(
+        buf, a,
+        [&](int b, int t, C v) {
+            if (b < cnt)
+                S[(size_t)t * cols + c0 + b] = v;
+        },
+        tw, tl, tid);
 }
 
 // ---------------------------------------------------------------------------
 // Y lines (one x plane per blockIdx.y; z-column tiles along blockIdx.x)
 // ---------------------------------------------------------------------------
-template <class R, int NY, int SIGN, bool KIN>
-__global__ void __launch_bounds__(256, 4)
-    k2_y(cplx<R> *__restrict__ psi, cplx<R> *__restrict__ S, int nz, int nblk_kin, Twid tk, Twid td) {
-    using C          = cplx<R>;
-    constexpr int NT = 256;
-    const int tid    = threadIdx.x;
-    const int i      = blockIdx.y;
-    C *b0            = reinterpret_cast<C *>(g_smem);
-    if (KIN && (int)blockIdx.x < nblk_kin) {
-        constexpr int CY = tile_lines<R, NY>() < 16 ? tile_lines<R, NY>() : 16;
-        const int k0     = blockIdx.x * CY;
-        const int cnt    = min(CY, nz - k0);
-        C *plane         = psi + (size_t)i * NY * nz;
-#pragma unroll 4
-        for (int e = tid; e < CY * NY; e += NT) {
-            const int j = e / CY, b = e % CY;
-            b0[b + j * CY] = b < cnt ? plane[(size_t)j * nz + k0 + b] : C{(R)0, (R)0};
-        }
-        __syncthreads();
-        ct_fft_ip<SIGN, R, NY, CY, CY, NT>(b0, (const C *)tk.tw, (const C *)tk.lo, tid);
-#pragma unroll 4
-        for (int e = tid; e < CY * NY; e += NT) {
-            const int j = e / CY, b = e % CY;
+template <class R, int NY, int SIGN, int CNT, int NT>
+__global__ void __launch_bounds__(NT) k3_y_kin(cplx<R> *__restrict__ psi, int nz, Twid tk) {
+    using C       = cplx<R>;
+    using P       = LinePass<SIGN, R, NY, CNT, CNT, NT, true, false>;
+    const int k0  = blockIdx.x * CNT;
+    const int cnt = min(CNT, nz - k0);
+    C *plane      = psi + (size_t)blockIdx.y * NY * nz + k0;
+    P::run(
+        reinterpret_cast<C *>(g_smem),
+        [&](int b, int t) { return b < cnt ? plane[(size_t)t * nz + b] : C{(R)0, (R)0}; },
+        [&](int b, int t, C v) {
             if (b < cnt)
-                plane[(size_t)j * nz + k0 + b] = b0[b + j * CY];
-        }
-        return;
-    }
-    constexpr int L  = 2 * NY;
-    constexpr int CD = tile_lines<R, L>() < 16 ? tile_lines<R, L>() : 16;
-    const int k0     = ((int)blockIdx.x - (KIN ? nblk_kin : 0)) * CD;
-    const int cnt    = min(CD, nz - k0);
-    C *plane         = S + (size_t)i * L * nz;
-    if (SIGN < 0) {
-        // rows NY..L-1 are the zero padding (not read by the pruned first stage)
-#pragma unroll 4
-        for (int e = tid; e < CD * NY; e += NT) {
-            const int j = e / CD, b = e % CD;
-            b0[b + j * CD] = b < cnt ? plane[(size_t)j * nz + k0 + b] : C{(R)0, (R)0};
-        }
-    } else {
-#pragma unroll 4
-        for (int e = tid; e < CD * L; e += NT) {
-            const int j = e / CD, b = e % CD;
-            b0[b + j * CD] = b < cnt ? plane[(size_t)j * nz + k0 + b] : C{(R)0, (R)0};
-        }
-    }
-    __syncthreads();
-    ct_fft_ip<SIGN, R, L, CD, CD, NT, false, (SIGN < 0), (SIGN > 0)>(b0, (const C *)td.tw, (const C *)td.lo,
-                                                                     tid);
-    const int rows_out = SIGN < 0 ? L : NY;
-    for (int e = tid; e < CD * rows_out; e += NT) {
-        const int j = e / CD, b = e % CD;
-        if (b < cnt)
-            plane[(size_t)j * nz + k0 + b] = b0[b + j * CD];
-    }
+                plane[(size_t)t * nz + b] = v;
+        },
+        (const C *)tk.tw, (const C *)tk.lo, threadIdx.x);
 }
+
+// Dipolar y lines of length 2ny: forward (SIGN < 0) with the upper half of the
+// input zero, inverse (SIGN > 0) with only the lower half of the output kept.
+template <class R, int NY, int SIGN, int CNT, int NT>
+__global__ void __launch_bounds__(NT) k3_y_dip(cplx<R> *__restrict__ S, int nz, Twid td) {
+    using C         = cplx<R>;
+    constexpr int L = 2 * NY;
+    using P         = LinePass<SIGN, R, L, CNT, CNT, NT, false, (SIGN > 0), (SIGN < 0), (SIGN > 0)>;
+    const int k0    = blockIdx.x * CNT;
+    const int cnt   = min(CNT, nz - k0);
+    C *plane        = S + (size_t)blockIdx.y * L * nz + k0;
+    P::run(
+        reinterpret_cast<C *>(g_smem),
+        [&](int b, int t) { return b < cnt ? plane[(size_t)t * nz + b] : C{(R)0, (R)0}; },
+        [&](int b, int t, C v) {
+            if (b < cnt)
+                plane[(size_t)t * nz + b] = v;
+        },
+        (const C *)td.tw, (const C *)td.lo, threadIdx.x);
+}
+
+// Shared memory of the x / y passes (one tile of COUNT lines).
+template <class R, int L, int CNT> constexpr size_t xy_smem() { return sizeof(cplx<R>) * CNT * L; }
+
+// Launch shapes of the x pass for nx = N: kinetic (CK lines, NTK threads) and
+// dipolar (CD lines of 2N, NTD threads).
+template <class R, int N> struct XShape {
+    static constexpr int CK = xy_count<N>(), NTK = pass_threads<N, CK>();
+    static constexpr int CD = xy_count<2 * N>(), NTD = pass_threads<2 * N, CD>();
+    static constexpr size_t SK = xy_smem<R, N, CK>(), SD = xy_smem<R, 2 * N, CD>();
+};
+// y pass for ny = N with CNT z columns per tile.
+template <class R, int N, int CNT> struct YShape {
+    static constexpr int NTK = pass_threads<N, CNT>(), NTD = pass_threads<2 * N, CNT>();
+    static constexpr size_t SK = xy_smem<R, N, CNT>(), SD = xy_smem<R, 2 * N, CNT>();
+};
 
 // ---------------------------------------------------------------------------
 // Z rows

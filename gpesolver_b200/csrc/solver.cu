@@ -575,21 +575,6 @@ template <class R> class Solver final : public SolverBase {
 
     static Twid twid(const Line &l) { return Twid{l.plan.tw, l.plan.twlo}; }
 
-    template <int N> static constexpr size_t x_smem(bool kin) {
-        const size_t k = kin ? (size_t)tile_lines<R, N>() * N : 0;
-        const size_t d = (size_t)tile_lines<R, 2 * N>() * 2 * N;
-        return sizeof(C) * (k > d ? k : d);
-    }
-    template <int N> static constexpr int y_ck() { return tile_lines<R, N>() < 16 ? tile_lines<R, N>() : 16; }
-    template <int N> static constexpr int y_cd() {
-        return tile_lines<R, 2 * N>() < 16 ? tile_lines<R, 2 * N>() : 16;
-    }
-    template <int N> static constexpr size_t y_smem(bool kin) {
-        const size_t k = kin ? (size_t)y_ck<N>() * N : 0;
-        const size_t d = (size_t)y_cd<N>() * 2 * N;
-        return sizeof(C) * (k > d ? k : d);
-    }
-
 #define GPE_XY_CASES(M) M(32) M(64) M(96) M(128) M(256)
 #define GPE_Z_CASES(M) M(8) M(16) M(24) M(32) M(64)
 
@@ -601,15 +586,19 @@ template <class R> class Solver final : public SolverBase {
             };
 #define GPE_SETX(N)                                                                                \
     if (nx == N) {                                                                                 \
-        set((const void *)k2_x<R, N, true>, x_smem<N>(true));                                       \
-        set((const void *)k2_x<R, N, false>, x_smem<N>(false));                                     \
+        using X = XShape<R, N>;                                                                    \
+        set((const void *)k3_x_kin<R, N, X::CK, X::NTK>, X::SK);                                   \
+        set((const void *)k3_x_dip<R, N, X::CD, X::NTD>, X::SD);                                   \
+    }
+#define GPE_SETY1(N, CNT, SIGN)                                                                    \
+    {                                                                                              \
+        using Y = YShape<R, N, CNT>;                                                               \
+        set((const void *)k3_y_kin<R, N, SIGN, CNT, Y::NTK>, Y::SK);                               \
+        set((const void *)k3_y_dip<R, N, SIGN, CNT, Y::NTD>, Y::SD);                               \
     }
 #define GPE_SETY(N)                                                                                \
     if (ny == N) {                                                                                 \
-        set((const void *)k2_y<R, N, -1, true>, y_smem<N>(true));                                   \
-        set((const void *)k2_y<R, N, +1, true>, y_smem<N>(true));                                   \
-        set((const void *)k2_y<R, N, -1, false>, y_smem<N>(false));                                 \
-        set((const void *)k2_y<R, N, +1, false>, y_smem<N>(false));                                 \
+        GPE_SETY1(N, 8, -1) GPE_SETY1(N, 8, +1) GPE_SETY1(N, 16, -1) GPE_SETY1(N, 16, +1)          \
     }
 #define GPE_SETZ(N)                                                                                \
     if (nz == N) {                                                                                 \
@@ -623,58 +612,55 @@ template <class R> class Solver final : public SolverBase {
             GPE_XY_CASES(GPE_SETY)
             GPE_Z_CASES(GPE_SETZ)
 #undef GPE_SETX
+#undef GPE_SETY1
 #undef GPE_SETY
 #undef GPE_SETZ
         }
     }
 
     // part: 0 both, 1 kinetic only, 2 dipolar only
+    // X pass: kinetic pencils (kin, part 0 or 1) and dipolar pencils (part 0, or !kin).
     void f_x(cudaStream_t s, bool kin, const double *divisor, int part = 0) {
         if constexpr (std::is_same<R, float>::value) {
             const double dscale = 1.0 / (8.0 * (double)N);
 #define GPE_LX(NN)                                                                                 \
     if (nx == NN) {                                                                                \
-        constexpr int CK = tile_lines<R, NN>(), CD = tile_lines<R, 2 * NN>();                     \
-        const int nk = kin ? (ny * nz + CK - 1) / CK : 0;                                          \
-        const int nd = (2 * ny * nz + CD - 1) / CD;                                                \
-        if (kin && part == 1)                                                                      \
-            launch(k2_x<R, NN, true>, nk, 256, x_smem<NN>(true), s, psi.p, S2.p, (const R *)vk2.p,   \
-                   (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, divisor, dscale, \
-                   ny, nz, nk, twid(kx), twid(dx));                                                \
-        else if (kin && part == 0)                                                                 \
-            launch(k2_x<R, NN, true>, nk + nd, 256, x_smem<NN>(true), s, psi.p, S2.p, (const R *)vk2.p, \
-                   (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, divisor, dscale, \
-                   ny, nz, nk, twid(kx), twid(dx));                                                \
-        else                                                                                       \
-            launch(k2_x<R, NN, false>, nd, 256, x_smem<NN>(false), s, psi.p, S2.p, (const R *)vk2.p, \
-                   (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, divisor, dscale, \
-                   ny, nz, 0, twid(kx), twid(dx));                                                 \
+        using X = XShape<R, NN>;                                                                   \
+        if (kin)                                                                                   \
+            launch(k3_x_kin<R, NN, X::CK, X::NTK>, (ny * nz + X::CK - 1) / X::CK, X::NTK, X::SK, s,  \
+                   psi.p, (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, ny, nz,  \
+                   twid(kx));                                                                      \
+        if (!kin || part == 0)                                                                     \
+            launch(k3_x_dip<R, NN, X::CD, X::NTD>, (2 * ny * nz + X::CD - 1) / X::CD, X::NTD, X::SD, \
+                   s, S2.p, (const R *)vk2.p, divisor, dscale, ny, nz, twid(dx));                  \
     }
             GPE_XY_CASES(GPE_LX)
 #undef GPE_LX
         }
     }
 
+    // Y pass (SIGN < 0 forward, > 0 inverse): kinetic lines (kin, part 0 or 1)
+    // and dipolar lines (part 0, or !kin).  Tiles of 16 z columns (8 when nz = 8).
     template <int SIGN> void f_y(cudaStream_t s, bool kin, int part = 0) {
         if constexpr (std::is_same<R, float>::value) {
+            if (nz >= 16)
+                f_y_cnt<SIGN, 16>(s, kin, part);
+            else
+                f_y_cnt<SIGN, 8>(s, kin, part);
+        }
+    }
+    template <int SIGN, int CNT> void f_y_cnt(cudaStream_t s, bool kin, int part) {
+        const dim3 grid((nz + CNT - 1) / CNT, nx);
 #define GPE_LY(NN)                                                                                 \
     if (ny == NN) {                                                                                \
-        constexpr int CK = y_ck<NN>(), CD = y_cd<NN>();                                            \
-        const int nk = kin ? (nz + CK - 1) / CK : 0;                                               \
-        const int nd = (nz + CD - 1) / CD;                                                         \
-        if (kin && part == 1)                                                                      \
-            launch(k2_y<R, NN, SIGN, true>, dim3(nk, nx), 256, y_smem<NN>(true), s, psi.p, S2.p, nz, nk, \
-                   twid(ky), twid(dy));                                                            \
-        else if (kin && part == 0)                                                                 \
-            launch(k2_y<R, NN, SIGN, true>, dim3(nk + nd, nx), 256, y_smem<NN>(true), s, psi.p, S2.p, \
-                   nz, nk, twid(ky), twid(dy));                                                    \
-        else                                                                                       \
-            launch(k2_y<R, NN, SIGN, false>, dim3(nd, nx), 256, y_smem<NN>(false), s, psi.p, S2.p, nz, \
-                   0, twid(ky), twid(dy));                                                         \
+        using Y = YShape<R, NN, CNT>;                                                              \
+        if (kin)                                                                                   \
+            launch(k3_y_kin<R, NN, SIGN, CNT, Y::NTK>, grid, Y::NTK, Y::SK, s, psi.p, nz, twid(ky)); \
+        if (!kin || part == 0)                                                                     \
+            launch(k3_y_dip<R, NN, SIGN, CNT, Y::NTD>, grid, Y::NTD, Y::SD, s, S2.p, nz, twid(dy));  \
     }
-            GPE_XY_CASES(GPE_LY)
+        GPE_XY_CASES(GPE_LY)
 #undef GPE_LY
-        }
     }
 
     template <int MODE> void f_z(cudaStream_t s, C *pin, C *pout, const StepCoef *coef, int local) {
@@ -1354,7 +1340,7 @@ int gpe_time_kernel(gpe_handle *h, int which, int reps, double *ms, double *byte
 const char *gpe_kernel_name(int which) {
     static const char *names[] = {"k_dip_z_fwd", "k_dip_y", "k_dip_x", "k_dip_y", "k_dip_z_inv",
                                   "k_kin_z", "k_kin_y", "k_kin_x", "k_kin_y", "k_kin_z",
-                                  "k_phase", "k_it_update", "k2_x", "k2_y", "k2_z", "k2_y"};
+                                  "k_phase", "k_it_update", "k3_x", "k3_y", "k2_z", "k3_y"};
     if (which < 0 || which >= GPE_K_COUNT)
         return "";
     return names[which];
