@@ -352,17 +352,29 @@ def run_our_arm(args):
 
     # ---- per-kernel roofline (kernels timed alone) ---------------------------
     # kernels of one RT iteration in the schedule the solver uses
-    per_step_count = {"F_X": 1, "F_YINV": 1, "F_Z": 1, "F_YFWD": 1}
+    # (plane-kernel grids: x pencils kinetic + dipolar, then the yz plane kernel;
+    # other fused grids: x pass, y inverse, z rows, y forward)
     L = capi.lib()
     kt = {}
     import ctypes
 
-    for idx, name in enumerate(capi.KERNELS):
-        if name not in per_step_count:
-            continue
-        ms, by = ctypes.c_double(), ctypes.c_double()
-        capi.check(L.gpe_time_kernel(solver.handle, idx, 200, ctypes.byref(ms), ctypes.byref(by)))
-        kt[name] = (ms.value, by.value, L.gpe_kernel_name(idx).decode())
+    def time_kernels(names):
+        for name in names:
+            idx = capi.KERNELS.index(name)
+            ms, by = ctypes.c_double(), ctypes.c_double()
+            rc = L.gpe_time_kernel(solver.handle, idx, 200, ctypes.byref(ms), ctypes.byref(by))
+            if rc != 0:
+                return False
+            kt[name] = (ms.value, by.value, L.gpe_kernel_name(idx).decode())
+        return True
+
+    if time_kernels(["F_YZ", "F_XK", "F_XD"]):
+        per_step_count = {"F_XK": 1, "F_XD": 1, "F_YZ": 1}
+    else:
+        kt.clear()
+        per_step_count = {"F_X": 1, "F_YINV": 1, "F_Z": 1, "F_YFWD": 1}
+        if not time_kernels(list(per_step_count)):
+            raise RuntimeError(capi.lib().gpe_last_error().decode())
     dom = max(per_step_count, key=lambda k: per_step_count[k] * kt[k][0])
     ms, by, kname = kt[dom]
     peak, peak_kind = measured_peak()

@@ -95,7 +95,8 @@ SIGNATURES = [
 GPE_NOALLOC_SCRATCH_BYTES = 16 << 20
 
 KERNELS = ["DIP_Z_FWD", "DIP_Y_FWD", "DIP_X", "DIP_Y_INV", "DIP_Z_INV", "KIN_Z_FWD", "KIN_Y_FWD",
-           "KIN_X", "KIN_Y_INV", "KIN_Z_INV", "PHASE", "IT_UPDATE", "F_X", "F_YINV", "F_Z", "F_YFWD"]
+           "KIN_X", "KIN_Y_INV", "KIN_Z_INV", "PHASE", "IT_UPDATE", "F_X", "F_YINV", "F_Z", "F_YFWD",
+           "F_XK", "F_XD", "F_YZ"]
 
 
 def lib() -> ctypes.CDLL:

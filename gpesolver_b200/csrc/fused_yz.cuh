@@ -1,0 +1,554 @@
+// One kernel per x plane for everything between two x passes.
+//
+// After the x pass, each x plane of psi (ny x nz, ky kz spectrum) and of the
+// dipolar spectrum (2ny x nz) is independent of the others until the next x
+// pass.  k4_yz keeps one plane of each in shared memory and runs, for plane i,
+//
+//   dipolar  iFFT_y(2ny, lower half kept) -> C2R_z (row pairs) -> phi
+//   kinetic  iFFT_y(ny) -> iFFT_z(nz) -> phase -> FFT_z(nz) -> FFT_y(ny)
+//   dipolar  rho -> R2C_z (row pairs) -> FFT_y(2ny, upper half zero)
+//
+// (imaginary time: the Euler stencil step in place of the kinetic transforms),
+// so one iteration is two kernels (x pass, yz plane) instead of four; the three
+// plane passes no longer go through global memory between each other.  The
+// z-line transforms pair through registers (iFFT_z ends, the phase is applied,
+// FFT_z starts, without a shared-memory round trip).
+//
+// Shared memory (complex C = 8 bytes in FP32), row stride PS = nz + 1 (odd:
+// conflict-free for both the y columns and the z rows):
+//   SP  2ny rows x PS  dipolar plane (ky or y, kz - 1)
+//   PP   ny rows x PS  psi plane (ky or y, kz or z)            (real time)
+//   FP   ny rows x (nz+1) reals: V + cdd phi, then rho
+//   DP  2nz x (ny/2 + 1): the row-pair lines of the real transforms; it shares
+//       the upper half of SP, which holds nothing between the pruned inverse y
+//       transform and the pruned forward one.
+#pragma once
+
+#include "fused.cuh"
+
+namespace gpe {
+
+// Barrier of a group of NTG threads: BAR = 0 is the whole block, BAR > 0 a
+// named barrier shared by the warps of one group.
+template <int BAR, int NTG> __device__ __forceinline__ void group_sync() {
+    if constexpr (BAR == 0)
+        __syncthreads();
+    else
+        asm volatile("bar.sync %0, %1;" ::"n"(BAR), "n"(NTG) : "memory");
+}
+
+// All stages of a transform over a tile in shared memory, in place (each stage
+// reads its butterflies into registers, synchronises, writes, synchronises).
+// Element t of line b at buf[b*BS + t*TS].  NT threads of barrier group BAR
+// take part (tid = index within the group).
+template <int SIGN, class R, int L, int COUNT, int BS, int TS, int NT, bool CMP, bool REV, bool IH = false,
+          bool OH = false, int BAR = 0>
+struct PlanePass {
+    using C                      = cplx<R>;
+    static constexpr Radices RAD = REV ? reversed(radices_of(L)) : radices_of(L);
+    static constexpr int NSTG    = RAD.n;
+
+    static constexpr int ns_before(int S) {
+        int ns = 1;
+        for (int s = 0; s < S; ++s)
+            ns *= RAD.r[s];
+        return ns;
+    }
+
+    template <int S> struct Stage {
+        static constexpr int RADIX  = RAD.r[S];
+        static constexpr int NS     = ns_before(S);
+        static constexpr int NR     = L / RADIX;
+        static constexpr int STEP   = L / (NS * RADIX);
+        static constexpr int ITEMS  = COUNT * NR;
+        static constexpr int ROUNDS = (ITEMS + NT - 1) / NT;
+        static constexpr bool PIN   = IH && S == 0;
+        static constexpr bool POUT  = OH && S == NSTG - 1;
+        static_assert(!PIN || RADIX % 2 == 0, "input pruning needs an even first radix");
+        static_assert(!POUT || RADIX % 2 == 0, "output pruning needs an even last radix");
+        using Regs = C[ROUNDS][RADIX];
+
+        static __device__ __forceinline__ bool valid(int it) { return ITEMS % NT == 0 || it < ITEMS; }
+
+        // butterfly inputs (twiddled) -> DFT, in registers
+        static __device__ __forceinline__ void read(const C *buf, Regs &a, const C *tw, const C *twlo,
+                                                    int tid) {
+#pragma unroll
+            for (int rd = 0; rd < ROUNDS; ++rd) {
+                const int it = rd * NT + tid;
+                if (!valid(it))
+                    break;
+                const int j  = it / COUNT;
+                const int b  = it - j * COUNT;
+                const int jm = j % NS;
+                const C *s   = buf + b * BS + j * TS;
+#pragma unroll
+                for (int k = 0; k < RADIX; ++k) {
+                    if (PIN && 2 * k >= RADIX) {
+                        a[rd][k] = C{(R)0, (R)0};
+                        continue;
+                    }
+                    C v = s[k * NR * TS];
+                    if (NS > 1 && k > 0) {
+                        const int t = jm * k * STEP;
+                        const C w   = __ldg(&tw[t]);
+                        if constexpr (sizeof(R) == 4 && CMP)
+                            v = twmul<SIGN>(v, w, __ldg(&twlo[t]));
+                        else
+                            v = SIGN < 0 ? cmul(v, w) : cmulc(v, w);
+                    }
+                    a[rd][k] = v;
+                }
+                DFTZ<RADIX, SIGN, R, CMP, PIN ? RADIX / 2 : RADIX>::run(a[rd]);
+            }
+        }
+
+        static __device__ __forceinline__ void write(C *buf, const Regs &a, int tid) {
+#pragma unroll
+            for (int rd = 0; rd < ROUNDS; ++rd) {
+                const int it = rd * NT + tid;
+                if (!valid(it))
+                    break;
+                const int j    = it / COUNT;
+                const int b    = it - j * COUNT;
+                const int jm   = j % NS;
+                const int idxD = (j / NS) * NS * RADIX + jm;
+                C *d           = buf + b * BS + idxD * TS;
+#pragma unroll
+                for (int q = 0; q < RADIX; ++q)
+                    if (!(POUT && 2 * q >= RADIX))
+                        d[q * NS * TS] = a[rd][q];
+            }
+        }
+
+        // line and element of output q of round rd
+        static __device__ __forceinline__ int line(int tid, int rd) { return (rd * NT + tid) % COUNT; }
+        static __device__ __forceinline__ int elem(int tid, int rd, int q) {
+            const int j = (rd * NT + tid) / COUNT;
+            return (j / NS) * NS * RADIX + j % NS + q * NS;
+        }
+    };
+
+    template <int S, int SE> static __device__ __forceinline__ void stages(C *buf, const C *tw, const C *twlo, int tid) {
+        if constexpr (S < SE) {
+            typename Stage<S>::Regs a;
+            Stage<S>::read(buf, a, tw, twlo, tid);
+            group_sync<BAR, NT>();
+            Stage<S>::write(buf, a, tid);
+            group_sync<BAR, NT>();
+            stages<S + 1, SE>(buf, tw, twlo, tid);
+        }
+    }
+
+    using Last  = Stage<NSTG - 1>;
+    using First = Stage<0>;
+
+    // The whole transform.  The tile must be complete (caller synchronised);
+    // returns after a final synchronisation.
+    static __device__ __forceinline__ void run(C *buf, const C *tw, const C *twlo, int tid) {
+        stages<0, NSTG>(buf, tw, twlo, tid);
+    }
+    // All stages but the writes of the last one: a = outputs of the last stage,
+    // Last::line / Last::elem give their positions.  Other threads may still
+    // read the tile: synchronise before writing it.
+    static __device__ __forceinline__ void run_to_regs(C *buf, typename Last::Regs &a, const C *tw,
+                                                       const C *twlo, int tid) {
+        stages<0, NSTG - 1>(buf, tw, twlo, tid);
+        Last::read(buf, a, tw, twlo, tid);
+    }
+    // Starts from the first stage's inputs in registers, laid out as
+    // run_to_regs of the reversed transform leaves them (same thread mapping).
+    // The tile must be free (caller synchronised).
+    static __device__ __forceinline__ void run_from_regs(C *buf, typename First::Regs &a, const C *tw,
+                                                         const C *twlo, int tid) {
+        static_assert(First::NS == 1, "first stage");
+#pragma unroll
+        for (int rd = 0; rd < First::ROUNDS; ++rd) {
+            if (!First::valid(rd * NT + tid))
+                break;
+            DFT<First::RADIX, SIGN, R, CMP>::run(a[rd]);
+        }
+        First::write(buf, a, tid);
+        group_sync<BAR, NT>();
+        stages<1, NSTG>(buf, tw, twlo, tid);
+    }
+};
+
+struct YZTwid {
+    Twid ky, kz, dy, dz;
+};
+
+// Global plane (ROWS x COLS complex, contiguous) <-> shared tile with row stride
+// PS.  Each thread issues all its 16-byte loads before any shared store.
+template <class R, int ROWS, int COLS, int PS, int NT>
+__device__ __forceinline__ void plane_in(cplx<R> *__restrict__ dst, const cplx<R> *__restrict__ src, int tid) {
+    using C          = cplx<R>;
+    static_assert(COLS % 2 == 0 && sizeof(C) == 8, "pairs of complex64 per 16-byte load");
+    constexpr int N2 = ROWS * COLS / 2;
+    constexpr int PER = (N2 + NT - 1) / NT;
+    const float4 *s4 = reinterpret_cast<const float4 *>(src);
+    float4 v[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+        const int e = u * NT + tid;
+        if (N2 % NT == 0 || e < N2)
+            v[u] = __ldg(&s4[e]);
+    }
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+        const int e = u * NT + tid;
+        if (N2 % NT == 0 || e < N2) {
+            const int r = (2 * e) / COLS, k = 2 * e - r * COLS;
+            dst[r * PS + k]     = C{v[u].x, v[u].y};
+            dst[r * PS + k + 1] = C{v[u].z, v[u].w};
+        }
+    }
+}
+template <class R, int ROWS, int COLS, int PS, int NT>
+__device__ __forceinline__ void plane_out(cplx<R> *__restrict__ dst, const cplx<R> *__restrict__ src, int tid) {
+    static_assert(COLS % 2 == 0 && sizeof(cplx<R>) == 8, "pairs of complex64 per 16-byte store");
+    constexpr int N2 = ROWS * COLS / 2;
+    float4 *d4       = reinterpret_cast<float4 *>(dst);
+#pragma unroll 4
+    for (int e = tid; e < N2; e += NT) {
+        const int r = (2 * e) / COLS, k = 2 * e - r * COLS;
+        const cplx<R> a = src[r * PS + k], b = src[r * PS + k + 1];
+        d4[e]           = make_float4(a.x, a.y, b.x, b.y);
+    }
+}
+
+// Plane-kernel geometry for ny = NY, nz = NZ.
+template <class R, int NY, int NZ> struct YZShape {
+    using C                      = cplx<R>;
+    static constexpr int PS      = NZ + 1;           // complex row stride of SP, PP
+    static constexpr int FS      = NZ + 1;           // real row stride of FP
+    static constexpr int NP      = NY / 2;           // row pairs
+    static constexpr int LD      = 2 * NZ;           // real-transform line length
+    static constexpr int TD      = NP + 1;           // DP element stride
+    static constexpr bool ALIAS  = LD * TD <= NY * PS; // DP fits in the upper half of SP
+    static constexpr size_t SP_B = sizeof(C) * 2 * NY * PS;
+    static constexpr size_t PP_B = sizeof(C) * NY * PS;
+    static constexpr size_t FP_B = sizeof(R) * NY * FS;
+    static constexpr size_t DP_B = ALIAS ? 0 : sizeof(C) * LD * TD;
+    static constexpr size_t SMEM = SP_B + PP_B + FP_B + DP_B;
+    static constexpr int NT0     = 2 * NY * NZ / 16;
+    static constexpr int NT      = NT0 < 128 ? 128 : (NT0 > 512 ? 512 : (NT0 + 31) / 32 * 32);
+    // Real time, SPLIT: the first ND threads run the dipolar chain while the
+    // other NK run the kinetic one (named barriers 1 and 2), meeting for phi
+    // and rho.  Measured slower at 128 x 128 x 32 (each chain then runs on half
+    // the warps), so every thread runs both chains one after the other.
+    static constexpr bool SPLIT  = false;
+    static constexpr int ND0     = (NT * 5 / 8 + 31) / 32 * 32;
+    static constexpr int ND      = !SPLIT ? NT : (ND0 > NT - 32 ? NT - 32 : ND0);
+    static constexpr int KOFF    = SPLIT ? ND : 0;
+    static constexpr int NK      = NT - KOFF;
+    static constexpr int BARD    = SPLIT ? 1 : 0;
+    static constexpr int BARK    = SPLIT ? 2 : 0;
+};
+
+// The dipolar chain of a plane, run by NTG threads of barrier group BAR.
+template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
+    using C         = cplx<R>;
+    using G         = YZShape<R, NY, NZ>;
+    static constexpr int PS = G::PS, FS = G::FS, NP = G::NP, LD = G::LD, TD = G::TD;
+
+    // iFFT_y(2ny, lower half kept) of SP, C2R_z of the row pairs -> phi (global)
+    // and FP = V + cdd phi.  SP must be loaded (caller synchronised).
+    static __device__ __forceinline__ void inverse(C *SP, C *DP, R *FP, R *phi_g, const R *V_g, R cdd,
+                                                   const YZTwid &tw, int t) {
+        PlanePass<+1, R, 2 * NY, NZ, 1, PS, NTG, false, true, false, true, BAR>::run(
+            SP, (const C *)tw.dy.tw, (const C *)tw.dy.lo, t);
+        // pair lines: z[m] = X_a[m] + i X_b[m] over the full 2nz-point spectrum
+        // (bins 1..nz stored at kz - 1, bin 0 is zero, bins > nz by symmetry);
+        // DP may share SP's upper half (rows >= NY), which nothing reads any more
+        for (int e = t; e < NP * LD; e += NTG) {
+            const int p = e % NP, m = e / NP;
+            C z         = C{(R)0, (R)0};
+            if (m > 0) {
+                const int mm = m <= NZ ? m : LD - m;
+                const C xa   = SP[(2 * p) * PS + mm - 1];
+                const C xb   = SP[(2 * p + 1) * PS + mm - 1];
+                if (m == NZ)
+                    z = C{xa.x, xb.x}; // self-conjugate bin: real parts only
+                else if (m < NZ)
+                    z = C{xa.x - xb.y, xa.y + xb.x};
+                else
+                    z = C{xa.x + xb.y, xb.x - xa.y};
+            }
+            DP[p + m * TD] = z;
+        }
+        group_sync<BAR, NTG>();
+        PlanePass<+1, R, LD, NP, 1, TD, NTG, false, true, false, true, BAR>::run(DP, (const C *)tw.dz.tw,
+                                                                                (const C *)tw.dz.lo, t);
+        for (int e = t; e < NY * NZ; e += NTG) {
+            const int r = e / NZ, k = e - r * NZ;
+            const C zz  = DP[(r >> 1) + k * TD];
+            const R f   = (r & 1) ? zz.y : zz.x;
+            phi_g[e]    = f;
+            FP[r * FS + k] = __ldg(&V_g[e]) + cdd * f;
+        }
+    }
+
+    // rho (FP) -> R2C_z of the row pairs -> FFT_y(2ny, upper half zero) -> S (global).
+    // FP must be complete (caller synchronised).
+    static __device__ __forceinline__ void forward(C *SP, C *DP, const R *FP, C *S_g, const YZTwid &tw, int t) {
+        for (int e = t; e < NP * NZ; e += NTG) {
+            const int p = e % NP, m = e / NP;
+            DP[p + m * TD] = C{FP[(2 * p) * FS + m], FP[(2 * p + 1) * FS + m]};
+        }
+        group_sync<BAR, NTG>();
+        PlanePass<-1, R, LD, NP, 1, TD, NTG, false, false, true, false, BAR>::run(DP, (const C *)tw.dz.tw,
+                                                                                 (const C *)tw.dz.lo, t);
+        for (int e = t; e < NY * NZ; e += NTG) {
+            const int r = e / NZ, m = e - r * NZ + 1; // bins 1..nz
+            const int p = r >> 1;
+            const C zm  = DP[p + m * TD];
+            const C zc  = DP[p + (LD - m) * TD];
+            C x;
+            if ((r & 1) == 0)
+                x = C{(R)0.5 * (zm.x + zc.x), (R)0.5 * (zm.y - zc.y)}; // (Z_m + conj(Z_{L-m}))/2
+            else
+                x = C{(R)0.5 * (zm.y + zc.y), (R)0.5 * (zc.x - zm.x)}; // (Z_m - conj(Z_{L-m}))/(2i)
+            SP[r * PS + m - 1] = x;
+        }
+        group_sync<BAR, NTG>();
+        PlanePass<-1, R, 2 * NY, NZ, 1, PS, NTG, false, false, true, false, BAR>::run(
+            SP, (const C *)tw.dy.tw, (const C *)tw.dy.lo, t);
+        plane_out<R, 2 * NY, NZ, PS, NTG>(S_g, SP, t);
+    }
+};
+
+template <class R, int NY, int NZ, int MODE>
+__global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid tw) {
+    using C                = cplx<R>;
+    using G                = YZShape<R, NY, NZ>;
+    constexpr int NT       = G::NT;
+    constexpr int ND = G::ND, NK = G::NK;
+    constexpr int PS = G::PS, FS = G::FS;
+    constexpr bool RT      = MODE <= ZM_RT_EPI;
+    constexpr bool HAS_INV = (MODE == ZM_RT_MID || MODE == ZM_RT_EPI || MODE == ZM_IT_MID);
+    const int tid          = threadIdx.x;
+    const int i            = blockIdx.x; // x plane
+    const int nx           = a.nx;
+
+    C *SP  = reinterpret_cast<C *>(g_smem);
+    C *PP  = SP + 2 * NY * PS;
+    R *FP  = reinterpret_cast<R *>(PP + NY * PS);
+    C *DP  = G::ALIAS ? SP + NY * PS : reinterpret_cast<C *>(FP + NY * FS);
+    __shared__ double red[NT / 32];
+
+    C *S_g         = reinterpret_cast<C *>(a.S) + (size_t)i * 2 * NY * NZ;
+    const R *V_g   = reinterpret_cast<const R *>(a.V) + (size_t)i * NY * NZ;
+    R *phi_g       = reinterpret_cast<R *>(a.phi) + (size_t)i * NY * NZ;
+    C *P_o         = reinterpret_cast<C *>(a.psi_out) + (size_t)i * NY * NZ;
+    const R cdd    = (R)a.cdd;
+
+    // ---- load the planes ------------------------------------------------------
+    if (HAS_INV)
+        plane_in<R, 2 * NY, NZ, PS, NT>(SP, S_g, tid);
+    if (RT || MODE == ZM_IT_MID)
+        plane_in<R, NY, NZ, PS, NT>(PP, reinterpret_cast<const C *>(a.psi_in) + (size_t)i * NY * NZ, tid);
+    __syncthreads();
+
+    if constexpr (RT) {
+        // The dipolar chain (threads < ND) and the kinetic chain (threads >=
+        // KOFF) meet twice: for phi before the phase, for rho after it.
+        constexpr int BD = G::BARD, BK = G::BARK, KOFF = G::KOFF;
+        using DW = DipolarPlane<R, NY, NZ, ND, BD>;
+        using KY = PlanePass<+1, R, NY, NZ, 1, PS, NK, true, false, false, false, BK>;
+        using KYF = PlanePass<-1, R, NY, NZ, 1, PS, NK, true, false, false, false, BK>;
+        using ZI = PlanePass<+1, R, NZ, NY, PS, 1, NK, true, false, false, false, BK>;
+        using ZF = PlanePass<-1, R, NZ, NY, PS, 1, NK, true, true, false, false, BK>;
+        static_assert(ZI::Last::RADIX == ZF::First::RADIX && ZI::Last::ROUNDS == ZF::First::ROUNDS &&
+                          ZI::Last::ITEMS == ZF::First::ITEMS,
+                      "paired z transforms share the register layout");
+        const bool dgrp = tid < ND;   // every thread unless SPLIT
+        const bool kgrp = tid >= KOFF; // every thread unless SPLIT
+        const int tk    = tid - KOFF;
+        typename ZI::Last::Regs zr;
+        if (dgrp) {
+            if (HAS_INV) {
+                DW::inverse(SP, DP, FP, phi_g, V_g, cdd, tw, tid);
+            } else {
+                // prologue: phi of the previous calc_fi3d
+                for (int e = tid; e < NY * NZ; e += ND) {
+                    const int r = e / NZ, k = e - r * NZ;
+                    FP[r * FS + k] = __ldg(&V_g[e]) + cdd * phi_g[e];
+                }
+            }
+        }
+        if (kgrp && HAS_INV) {
+            KY::run(PP, (const C *)tw.ky.tw, (const C *)tw.ky.lo, tk);
+            ZI::run_to_regs(PP, zr, (const C *)tw.kz.tw, (const C *)tw.kz.lo, tk);
+        }
+        __syncthreads(); // FP = V + cdd phi
+
+        // merged potential half steps: theta = -dt/2 [cV (V + cdd phi) + g3 |psi|^2 + gw |psi|^3]
+        R cV, g3, gw;
+        {
+            const int base    = *a.step.base + a.step.local;
+            const StepCoef c0 = a.step.coef[base];
+            if (MODE == ZM_RT_MID) {
+                const StepCoef c1 = a.step.coef[base + 1];
+                cV                = (R)2;
+                g3                = (R)(c0.g3w + c1.g3w);
+                gw                = (R)(c0.gw15 + c1.gw15);
+            } else {
+                cV = (R)1;
+                g3 = (R)c0.g3w;
+                gw = (R)c0.gw15;
+            }
+        }
+        const R hdt = (R)a.half_dt, wat = (R)a.w_atoms;
+        const bool xin = i >= 1 && i < nx - 1;
+        auto phase = [&](C p, int y, int z) -> C {
+            const int f = y * FS + z;
+            if (xin && y >= 1 && y < NY - 1 && z >= 1 && z < NZ - 1) {
+                const R dens  = p.x * p.x + p.y * p.y;
+                const R am    = sqrt(dens);
+                const R total = cV * FP[f] + g3 * dens + gw * (am * am * am);
+                R s, c;
+                sincos_r<R>((R)-0.5 * hdt * total, &s, &c);
+                p = apply_wm1(p, C{(R)-2 * s * s, (R)2 * s * c});
+            }
+            FP[f] = wat * (p.x * p.x + p.y * p.y); // rho for the next dipolar spectrum
+            return p;
+        };
+        if (MODE == ZM_RT_PRO) {
+            // psi is in real space: every thread takes part in the phase
+            for (int e = tid; e < NY * NZ; e += NT) {
+                const int r = e / NZ, k = e - r * NZ;
+                PP[r * PS + k] = phase(PP[r * PS + k], r, k);
+            }
+        } else if (kgrp) {
+#pragma unroll
+            for (int rd = 0; rd < ZI::Last::ROUNDS; ++rd) {
+                if (!ZI::Last::valid(rd * NK + tk))
+                    break;
+                const int y = ZI::Last::line(tk, rd);
+#pragma unroll
+                for (int q = 0; q < ZI::Last::RADIX; ++q)
+                    zr[rd][q] = phase(zr[rd][q], y, ZI::Last::elem(tk, rd, q));
+            }
+            if (MODE == ZM_RT_EPI) {
+                // psi in real space -> global
+                group_sync<BK, NK>();
+                ZI::Last::write(PP, zr, tk);
+                group_sync<BK, NK>();
+                plane_out<R, NY, NZ, PS, NK>(P_o, PP, tk);
+            }
+        }
+        if (MODE == ZM_RT_EPI)
+            return;
+        __syncthreads(); // rho complete
+
+        if (dgrp)
+            DW::forward(SP, DP, FP, S_g, tw, tid);
+        if (kgrp) {
+            if (MODE == ZM_RT_PRO)
+                ZF::run(PP, (const C *)tw.kz.tw, (const C *)tw.kz.lo, tk);
+            else
+                ZF::run_from_regs(PP, zr, (const C *)tw.kz.tw, (const C *)tw.kz.lo, tk);
+            KYF::run(PP, (const C *)tw.ky.tw, (const C *)tw.ky.lo, tk);
+            plane_out<R, NY, NZ, PS, NK>(P_o, PP, tk);
+        }
+    } else {
+        using DW = DipolarPlane<R, NY, NZ, NT, 0>;
+        // imaginary time: psi_in / sqrt(divisor)
+        const C *__restrict__ pin = reinterpret_cast<const C *>(a.psi_in);
+        C *__restrict__ pout      = reinterpret_cast<C *>(a.psi_out);
+        const C *__restrict__ bnd = reinterpret_cast<const C *>(a.bnd);
+        const R sc        = (R)(1.0 / sqrt(a.norm_state[1]));
+        const R wat       = (R)a.w_atoms;
+        const size_t pln  = (size_t)NY * NZ;
+        const size_t base = (size_t)i * pln;
+        double acc        = 0.0;
+        if (MODE == ZM_IT_PRO) {
+            for (int e = tid; e < NY * NZ; e += NT) {
+                const int r = e / NZ, k = e - r * NZ;
+                const C p   = __ldg(&pin[base + e]);
+                FP[r * FS + k] = wat * (p.x * p.x + p.y * p.y);
+            }
+        } else {
+            DW::inverse(SP, DP, FP, phi_g, V_g, cdd, tw, tid);
+            __syncthreads(); // FP complete
+            const StepCoef cf = a.step.coef[0];
+            const R g3w = (R)cf.g3w, gw15 = (R)cf.gw15;
+            const R cx = (R)a.cx, cy = (R)a.cy, cz = (R)a.cz, dtau = (R)a.dtau;
+            const bool xin = i >= 1 && i < nx - 1;
+#pragma unroll 2
+            for (int e = tid; e < NY * NZ; e += NT) {
+                const int r = e / NZ, k = e - r * NZ;
+                const size_t q = base + e;
+                C o;
+                if (!xin || r < 1 || r >= NY - 1 || k < 1 || k >= NZ - 1) {
+                    o = __ldg(&bnd[q]);
+                } else {
+                    const C *pp = PP + r * PS + k; // this plane (shared), x neighbours (global)
+                    const C c0 = cscale(pp[0], sc);
+                    const C xm = cscale(__ldg(&pin[q - pln]), sc), xp = cscale(__ldg(&pin[q + pln]), sc);
+                    const C ym = cscale(pp[-PS], sc), yp = cscale(pp[PS], sc);
+                    const C zm = cscale(pp[-1], sc), zp = cscale(pp[1], sc);
+                    const R vv   = FP[r * FS + k];
+                    const R dens = c0.x * c0.x + c0.y * c0.y;
+                    const R am   = sqrt(dens);
+                    const R nl   = g3w * dens + gw15 * (am * am * am);
+                    const R lr   = cx * ((xm.x + xp.x) - 2 * c0.x) - cy * ((ym.x + yp.x) - 2 * c0.x) -
+                                 cz * ((zm.x + zp.x) - 2 * c0.x) + c0.x * vv + nl * c0.x;
+                    const R li = cx * ((xm.y + xp.y) - 2 * c0.y) - cy * ((ym.y + yp.y) - 2 * c0.y) -
+                                 cz * ((zm.y + zp.y) - 2 * c0.y) + c0.y * vv + nl * c0.y;
+                    o = C{c0.x - dtau * lr, c0.y - dtau * li};
+                }
+                pout[q] = o;
+                acc += (double)o.x * o.x + (double)o.y * o.y;
+                FP[r * FS + k] = wat * (o.x * o.x + o.y * o.y);
+            }
+        }
+        __syncthreads(); // rho complete; SP's upper half (DP) free
+        DW::forward(SP, DP, FP, S_g, tw, tid);
+
+        // ---- norm of psi' (imaginary time): deterministic two-level reduction -----
+        if (MODE == ZM_IT_MID) {
+            for (int off = 16; off > 0; off >>= 1)
+                acc += __shfl_down_sync(0xffffffffu, acc, off);
+            if ((tid & 31) == 0)
+                red[tid >> 5] = acc;
+            __syncthreads();
+            __shared__ bool last;
+            if (tid == 0) {
+                double v = 0;
+                for (int w = 0; w < NT / 32; ++w)
+                    v += red[w];
+                a.partial[blockIdx.x] = v;
+                __threadfence();
+                const unsigned t = atomicAdd(a.ticket, 1u);
+                last             = (t == gridDim.x - 1);
+            }
+            __syncthreads();
+            if (last) {
+                __threadfence();
+                double v = 0;
+                for (int b = tid; b < (int)gridDim.x; b += NT)
+                    v += ((volatile double *)a.partial)[b];
+                for (int off = 16; off > 0; off >>= 1)
+                    v += __shfl_down_sync(0xffffffffu, v, off);
+                if ((tid & 31) == 0)
+                    red[tid >> 5] = v;
+                __syncthreads();
+                if (tid == 0) {
+                    double x = 0;
+                    for (int w = 0; w < NT / 32; ++w)
+                        x += red[w];
+                    x *= a.dV;
+                    a.norm_state[0] = x;
+                    a.norm_state[1] = x;
+                    if (!(x > 0.0) || !isfinite(x))
+                        a.status[0] = 1;
+                    *a.ticket = 0u;
+                }
+            }
+        }
+    }
+}
+
+} // namespace gpe

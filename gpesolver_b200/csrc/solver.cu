@@ -6,7 +6,7 @@
 // waits where the reference's interface returns a value (norm, energies,
 // exported fields).
 #include "../../include/gpe_b200.h"
-#include "fused.cuh"
+#include "fused_yz.cuh"
 #include "kernels.cuh"
 #include "plan.hpp"
 
@@ -423,12 +423,19 @@ template <class R> class Solver final : public SolverBase {
             throw Error(GPE_ERR_ARG, "bad kernel id or repetition count");
         materialize();
         // save the state the kernels modify
-        DevBuf<C> save_psi, save_A;
+        DevBuf<C> save_psi, save_A, save_S2;
+        DevBuf<R> save_phi;
         save_psi.alloc(N);
         save_A.alloc(A.n);
+        save_phi.alloc(N);
         GPE_CUDA(cudaMemcpyAsync(save_psi.p, psi.p, sizeof(C) * N, cudaMemcpyDeviceToDevice, cur));
         GPE_CUDA(cudaMemcpyAsync(save_A.p, A.p, sizeof(C) * A.n, cudaMemcpyDeviceToDevice, cur));
-        if (which == GPE_K_F_Z) {
+        GPE_CUDA(cudaMemcpyAsync(save_phi.p, phi.p, sizeof(R) * N, cudaMemcpyDeviceToDevice, cur));
+        if (fused) {
+            save_S2.alloc(S2.n);
+            GPE_CUDA(cudaMemcpyAsync(save_S2.p, S2.p, sizeof(C) * S2.n, cudaMemcpyDeviceToDevice, cur));
+        }
+        if (which == GPE_K_F_Z || which == GPE_K_F_YZ) {
             // the merged phase reads the coefficients of two consecutive iterations
             ensure_coef_capacity(2);
             GPE_CUDA(cudaEventSynchronize(coef_event));
@@ -503,12 +510,27 @@ template <class R> class Solver final : public SolverBase {
             case GPE_K_F_X:
             case GPE_K_F_YINV:
             case GPE_K_F_Z:
-            case GPE_K_F_YFWD: {
+            case GPE_K_F_YFWD:
+            case GPE_K_F_XK:
+            case GPE_K_F_XD:
+            case GPE_K_F_YZ: {
                 if (!fused)
                     throw Error(GPE_ERR_STATE, "the fused pipeline is not available for this grid");
+                if (which == GPE_K_F_YZ && !yz_plane())
+                    throw Error(GPE_ERR_STATE, "no yz plane kernel for this grid");
                 const double S2b = (double)sizeof(C) * nx * 2 * ny * nz;
                 const double S2h = (double)sizeof(C) * nx * ny * nz;
-                if (which == GPE_K_F_X) {
+                if (which == GPE_K_F_XK) {
+                    f_x(cur, true, nullptr, 1);
+                    b = 2 * F; // psi spectrum in and out
+                } else if (which == GPE_K_F_XD) {
+                    f_x(cur, false, nullptr);
+                    b = 2 * S2h + (double)sizeof(R) * (nx + 1) * (ny + 1) * nz; // + the V_dd table
+                } else if (which == GPE_K_F_YZ) {
+                    f_yz<ZM_RT_MID>(cur, psi.p, psi.p, coef_dev.p, 0);
+                    // psi R+W, spectrum (2ny rows) R+W, V read, phi write
+                    b = 2 * F + 2 * S2b + Rb + Rb;
+                } else if (which == GPE_K_F_X) {
                     f_x(cur, true, nullptr);
                     b = 2 * F + 2 * S2h; // kinetic R+W; dipolar reads and writes nx of 2nx planes
                 } else if (which == GPE_K_F_YINV) {
@@ -541,6 +563,9 @@ template <class R> class Solver final : public SolverBase {
         cudaEventDestroy(e1);
         GPE_CUDA(cudaMemcpyAsync(psi.p, save_psi.p, sizeof(C) * N, cudaMemcpyDeviceToDevice, cur));
         GPE_CUDA(cudaMemcpyAsync(A.p, save_A.p, sizeof(C) * A.n, cudaMemcpyDeviceToDevice, cur));
+        GPE_CUDA(cudaMemcpyAsync(phi.p, save_phi.p, sizeof(R) * N, cudaMemcpyDeviceToDevice, cur));
+        if (fused)
+            GPE_CUDA(cudaMemcpyAsync(S2.p, save_S2.p, sizeof(C) * S2.n, cudaMemcpyDeviceToDevice, cur));
         GPE_CUDA(cudaStreamSynchronize(cur));
         *ms    = (double)t / reps;
         *bytes = b;
@@ -577,6 +602,7 @@ template <class R> class Solver final : public SolverBase {
 
 #define GPE_XY_CASES(M) M(32) M(64) M(96) M(128) M(256)
 #define GPE_Z_CASES(M) M(8) M(16) M(24) M(32) M(64)
+#define GPE_YZ_CASES(M) M(32, 16) M(64, 16) M(64, 32) M(96, 24) M(128, 32)
 
     void set_fused_attrs() {
         if constexpr (std::is_same<R, float>::value) {
@@ -608,6 +634,17 @@ template <class R> class Solver final : public SolverBase {
         set((const void *)k2_z<R, N, ZM_IT_PRO>, z_smem<R, N>());                                   \
         set((const void *)k2_z<R, N, ZM_IT_MID>, z_smem<R, N>());                                   \
     }
+#define GPE_SETYZ(A, B)                                                                            \
+    if (ny == A && nz == B) {                                                                      \
+        using G = YZShape<R, A, B>;                                                                \
+        set((const void *)k4_yz<R, A, B, ZM_RT_PRO>, G::SMEM);                                     \
+        set((const void *)k4_yz<R, A, B, ZM_RT_MID>, G::SMEM);                                     \
+        set((const void *)k4_yz<R, A, B, ZM_RT_EPI>, G::SMEM);                                     \
+        set((const void *)k4_yz<R, A, B, ZM_IT_PRO>, G::SMEM);                                     \
+        set((const void *)k4_yz<R, A, B, ZM_IT_MID>, G::SMEM);                                     \
+    }
+            GPE_YZ_CASES(GPE_SETYZ)
+#undef GPE_SETYZ
             GPE_XY_CASES(GPE_SETX)
             GPE_XY_CASES(GPE_SETY)
             GPE_Z_CASES(GPE_SETZ)
@@ -663,30 +700,35 @@ template <class R> class Solver final : public SolverBase {
 #undef GPE_LY
     }
 
+    ZArgs zargs(C *pin, C *pout, const StepCoef *coef, int local) {
+        ZArgs a{};
+        a.psi_in     = pin;
+        a.psi_out    = pout;
+        a.bnd        = bnd.p;
+        a.S          = S2.p;
+        a.V          = V.p;
+        a.phi        = phi.p;
+        a.norm_state = norm_state.p;
+        a.partial    = zpartial.p;
+        a.ticket     = ticket.p;
+        a.status     = status.p;
+        a.dV         = P.dx * P.dy * P.dz;
+        a.step       = StepIdx{coef, iter_base.p, local};
+        a.half_dt    = P.real_time_dt / 2.;
+        a.cdd        = P.cdd;
+        a.w_atoms    = P.n_atoms;
+        a.cx         = -0.5 / (P.m * P.dx * P.dx);
+        a.cy         = 0.5 / (P.m * P.dy * P.dy);
+        a.cz         = 0.5 / (P.m * P.dz * P.dz);
+        a.dtau       = P.imag_time_dt;
+        a.nx         = nx;
+        a.ny         = ny;
+        return a;
+    }
+
     template <int MODE> void f_z(cudaStream_t s, C *pin, C *pout, const StepCoef *coef, int local) {
         if constexpr (std::is_same<R, float>::value) {
-            ZArgs a{};
-            a.psi_in     = pin;
-            a.psi_out    = pout;
-            a.bnd        = bnd.p;
-            a.S          = S2.p;
-            a.V          = V.p;
-            a.phi        = phi.p;
-            a.norm_state = norm_state.p;
-            a.partial    = zpartial.p;
-            a.ticket     = ticket.p;
-            a.status     = status.p;
-            a.dV         = P.dx * P.dy * P.dz;
-            a.step       = StepIdx{coef, iter_base.p, local};
-            a.half_dt    = P.real_time_dt / 2.;
-            a.cdd        = P.cdd;
-            a.w_atoms    = P.n_atoms;
-            a.cx         = -0.5 / (P.m * P.dx * P.dx);
-            a.cy         = 0.5 / (P.m * P.dy * P.dy);
-            a.cz         = 0.5 / (P.m * P.dz * P.dz);
-            a.dtau       = P.imag_time_dt;
-            a.nx         = nx;
-            a.ny         = ny;
+            const ZArgs a  = zargs(pin, pout, coef, local);
             const int grid = (nx * ny + 31) / 32;
 #define GPE_LZ(NN)                                                                                 \
     if (nz == NN)                                                                                  \
@@ -696,9 +738,36 @@ template <class R> class Solver final : public SolverBase {
         }
     }
 
+    // The y passes and the z rows of one iteration as one kernel per x plane
+    // (grids whose ny x nz planes fit in shared memory).
+    bool yz_plane() const {
+        bool ok = false;
+#define GPE_YZOK(A, B) ok = ok || (ny == A && nz == B);
+        GPE_YZ_CASES(GPE_YZOK)
+#undef GPE_YZOK
+        return fused && ok;
+    }
+    template <int MODE> void f_yz(cudaStream_t s, C *pin, C *pout, const StepCoef *coef, int local) {
+        if constexpr (std::is_same<R, float>::value) {
+            const ZArgs a = zargs(pin, pout, coef, local);
+            const YZTwid t{twid(ky), twid(kz), twid(dy), twid(dz)};
+#define GPE_LYZ(A, B)                                                                              \
+    if (ny == A && nz == B) {                                                                      \
+        using G = YZShape<R, A, B>;                                                                \
+        launch(k4_yz<R, A, B, MODE>, nx, G::NT, G::SMEM, s, a, t);                                \
+    }
+            GPE_YZ_CASES(GPE_LYZ)
+#undef GPE_LYZ
+        }
+    }
+
     // kind 10: RT prologue; 11: C mid RT iterations; 12: `count` mid + the last;
     // kind 20: IT prologue; 21: `count` IT iterations.
     void capture_fused(int kind, int count) {
+        if (yz_plane()) {
+            capture_fused_yz(kind, count);
+            return;
+        }
         cudaStream_t s = cap_stream;
         if (kind == 10) {
             f_z<ZM_RT_PRO>(s, psi.p, psi.p, coef_dev.p, 0);
@@ -744,6 +813,43 @@ template <class R> class Solver final : public SolverBase {
                 f_y<+1>(s, false);
                 f_z<ZM_IT_MID>(s, a, b, cur_coef.p, 0);
                 f_y<-1>(s, false);
+                std::swap(a, b);
+            }
+        }
+    }
+
+    // Two kernels per iteration: x pass (kinetic and dipolar pencils as two graph
+    // branches in real time), then the yz plane kernel.
+    void capture_fused_yz(int kind, int count) {
+        cudaStream_t s = cap_stream;
+        if (kind == 10) {
+            f_yz<ZM_RT_PRO>(s, psi.p, psi.p, coef_dev.p, 0);
+        } else if (kind == 11 || kind == 12) {
+            cudaStream_t s2 = cap_stream2;
+            for (int t = 0; t <= count; ++t) {
+                if (t == count && kind == 11)
+                    break;
+                GPE_CUDA(cudaEventRecord(ev_fork, s));
+                GPE_CUDA(cudaStreamWaitEvent(s2, ev_fork, 0));
+                f_x(s, true, nullptr, 1);
+                f_x(s2, false, nullptr);
+                GPE_CUDA(cudaEventRecord(ev_join, s2));
+                GPE_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
+                if (t == count) {
+                    f_yz<ZM_RT_EPI>(s, psi.p, psi.p, coef_dev.p, count);
+                    break;
+                }
+                f_yz<ZM_RT_MID>(s, psi.p, psi.p, coef_dev.p, t);
+            }
+            if (kind == 11)
+                launch(k_advance, 1, 1, 0, s, iter_base.p, count);
+        } else if (kind == 20) {
+            f_yz<ZM_IT_PRO>(s, psi.p, psi.p, cur_coef.p, 0);
+        } else {
+            C *a = psi.p, *b = psii.p;
+            for (int t = 0; t < count; ++t) {
+                f_x(s, false, norm_state.p + 1);
+                f_yz<ZM_IT_MID>(s, a, b, cur_coef.p, 0);
                 std::swap(a, b);
             }
         }
@@ -1340,7 +1446,8 @@ int gpe_time_kernel(gpe_handle *h, int which, int reps, double *ms, double *byte
 const char *gpe_kernel_name(int which) {
     static const char *names[] = {"k_dip_z_fwd", "k_dip_y", "k_dip_x", "k_dip_y", "k_dip_z_inv",
                                   "k_kin_z", "k_kin_y", "k_kin_x", "k_kin_y", "k_kin_z",
-                                  "k_phase", "k_it_update", "k3_x", "k3_y", "k2_z", "k3_y"};
+                                  "k_phase", "k_it_update", "k3_x", "k3_y", "k2_z", "k3_y",
+                                  "k3_x_kin", "k3_x_dip", "k4_yz"};
     if (which < 0 || which >= GPE_K_COUNT)
         return "";
     return names[which];

@@ -157,6 +157,9 @@ enum {
     GPE_K_PHASE, GPE_K_IT_UPDATE,
     /* the fused pipeline (real time): X pencils, Y inverse, Z rows, Y forward */
     GPE_K_F_X, GPE_K_F_YINV, GPE_K_F_Z, GPE_K_F_YFWD,
+    /* kinetic x pencils alone, dipolar x pencils alone, the yz plane kernel
+       (grids with a plane kernel: one iteration = F_XK + F_XD + F_YZ) */
+    GPE_K_F_XK, GPE_K_F_XD, GPE_K_F_YZ,
     GPE_K_COUNT
 };
 /* Launches kernel `which` `reps` times back to back on the handle's stream
