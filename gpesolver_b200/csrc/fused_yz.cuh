@@ -148,6 +148,25 @@ struct PlanePass {
     static __device__ __forceinline__ void run(C *buf, const C *tw, const C *twlo, int tid) {
         stages<0, NSTG>(buf, tw, twlo, tid);
     }
+    // All stages, the last one handing its outputs to st(b, t, v) (element t of
+    // line b) instead of writing the tile.  Other threads may still read the
+    // tile on return: synchronise before reusing it.
+    template <class St>
+    static __device__ __forceinline__ void run_emit(C *buf, St st, const C *tw, const C *twlo, int tid) {
+        stages<0, NSTG - 1>(buf, tw, twlo, tid);
+        typename Last::Regs a;
+        Last::read(buf, a, tw, twlo, tid);
+#pragma unroll
+        for (int rd = 0; rd < Last::ROUNDS; ++rd) {
+            if (!Last::valid(rd * NT + tid))
+                break;
+            const int b = Last::line(tid, rd);
+#pragma unroll
+            for (int q = 0; q < Last::RADIX; ++q)
+                if (!(Last::POUT && 2 * q >= Last::RADIX))
+                    st(b, Last::elem(tid, rd, q), a[rd][q]);
+        }
+    }
     // All stages but the writes of the last one: a = outputs of the last stage,
     // Last::line / Last::elem give their positions.  Other threads may still
     // read the tile: synchronise before writing it.
@@ -177,6 +196,34 @@ struct PlanePass {
 struct YZTwid {
     Twid ky, kz, dy, dz;
 };
+
+// Asynchronous global -> shared copies (cp.async, no register staging).
+__device__ __forceinline__ void cp_async8(void *smem, const void *g) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *g) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most N of this thread's committed groups are pending
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+// ROWS x COLS plane (contiguous in global) -> shared rows of stride PS
+template <class T, int ROWS, int COLS, int PS, int NT>
+__device__ __forceinline__ void plane_in_async(T *dst, const T *src, int tid) {
+    static_assert(sizeof(T) == 8 || sizeof(T) == 4, "8- or 4-byte elements");
+#pragma unroll 4
+    for (int e = tid; e < ROWS * COLS; e += NT) {
+        const int r = e / COLS, k = e - r * COLS;
+        if constexpr (sizeof(T) == 8)
+            cp_async8(&dst[r * PS + k], &src[e]);
+        else
+            cp_async4(&dst[r * PS + k], &src[e]);
+    }
+}
 
 // Global plane (ROWS x COLS complex, contiguous) <-> shared tile with row stride
 // PS.  Each thread issues all its 16-byte loads before any shared store.
@@ -252,12 +299,16 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
     using G         = YZShape<R, NY, NZ>;
     static constexpr int PS = G::PS, FS = G::FS, NP = G::NP, LD = G::LD, TD = G::TD;
 
-    // iFFT_y(2ny, lower half kept) of SP, C2R_z of the row pairs -> phi (global)
-    // and FP = V + cdd phi.  SP must be loaded (caller synchronised).
-    static __device__ __forceinline__ void inverse(C *SP, C *DP, R *FP, R *phi_g, const R *V_g, R cdd,
-                                                   const YZTwid &tw, int t) {
+    // iFFT_y(2ny, lower half kept) of SP, C2R_z of the row pairs -> FP = V + cdd
+    // phi (FP holds V on entry), and phi -> global when WRITE_PHI.  SP must be
+    // loaded (caller synchronised); the caller's other cp.async group (psi, V)
+    // is waited for here, overlapped with the y transforms.
+    template <bool WRITE_PHI>
+    static __device__ __forceinline__ void inverse(C *SP, C *DP, R *FP, R *phi_g, R cdd, const YZTwid &tw,
+                                                   int t) {
         PlanePass<+1, R, 2 * NY, NZ, 1, PS, NTG, false, true, false, true, BAR>::run(
             SP, (const C *)tw.dy.tw, (const C *)tw.dy.lo, t);
+        cp_async_wait<0>(); // visible to the block after the next barrier
         // pair lines: z[m] = X_a[m] + i X_b[m] over the full 2nz-point spectrum
         // (bins 1..nz stored at kz - 1, bin 0 is zero, bins > nz by symmetry);
         // DP may share SP's upper half (rows >= NY), which nothing reads any more
@@ -284,8 +335,9 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
             const int r = e / NZ, k = e - r * NZ;
             const C zz  = DP[(r >> 1) + k * TD];
             const R f   = (r & 1) ? zz.y : zz.x;
-            phi_g[e]    = f;
-            FP[r * FS + k] = __ldg(&V_g[e]) + cdd * f;
+            if (WRITE_PHI)
+                phi_g[e] = f;
+            FP[r * FS + k] += cdd * f;
         }
     }
 
@@ -312,9 +364,8 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
             SP[r * PS + m - 1] = x;
         }
         group_sync<BAR, NTG>();
-        PlanePass<-1, R, 2 * NY, NZ, 1, PS, NTG, false, false, true, false, BAR>::run(
-            SP, (const C *)tw.dy.tw, (const C *)tw.dy.lo, t);
-        plane_out<R, 2 * NY, NZ, PS, NTG>(S_g, SP, t);
+        PlanePass<-1, R, 2 * NY, NZ, 1, PS, NTG, false, false, true, false, BAR>::run_emit(
+            SP, [&](int b, int r, C v) { S_g[r * NZ + b] = v; }, (const C *)tw.dy.tw, (const C *)tw.dy.lo, t);
     }
 };
 
@@ -343,11 +394,19 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     C *P_o         = reinterpret_cast<C *>(a.psi_out) + (size_t)i * NY * NZ;
     const R cdd    = (R)a.cdd;
 
-    // ---- load the planes ------------------------------------------------------
+    // ---- load the planes (two cp.async groups: S; psi and V) -------------------
     if (HAS_INV)
-        plane_in<R, 2 * NY, NZ, PS, NT>(SP, S_g, tid);
+        plane_in_async<C, 2 * NY, NZ, PS, NT>(SP, S_g, tid);
+    cp_async_commit();
     if (RT || MODE == ZM_IT_MID)
-        plane_in<R, NY, NZ, PS, NT>(PP, reinterpret_cast<const C *>(a.psi_in) + (size_t)i * NY * NZ, tid);
+        plane_in_async<C, NY, NZ, PS, NT>(PP, reinterpret_cast<const C *>(a.psi_in) + (size_t)i * NY * NZ, tid);
+    if (MODE != ZM_IT_PRO)
+        plane_in_async<R, NY, NZ, FS, NT>(FP, V_g, tid);
+    cp_async_commit();
+    if (HAS_INV)
+        cp_async_wait<1>(); // S; psi and V are waited for inside the dipolar inverse
+    else
+        cp_async_wait<0>();
     __syncthreads();
 
     if constexpr (RT) {
@@ -368,16 +427,21 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
         typename ZI::Last::Regs zr;
         if (dgrp) {
             if (HAS_INV) {
-                DW::inverse(SP, DP, FP, phi_g, V_g, cdd, tw, tid);
+                // phi is needed in global memory only after the last iteration
+                DW::template inverse<MODE != ZM_RT_MID>(SP, DP, FP, phi_g, cdd, tw, tid);
             } else {
                 // prologue: phi of the previous calc_fi3d
                 for (int e = tid; e < NY * NZ; e += ND) {
                     const int r = e / NZ, k = e - r * NZ;
-                    FP[r * FS + k] = __ldg(&V_g[e]) + cdd * phi_g[e];
+                    FP[r * FS + k] += cdd * phi_g[e];
                 }
             }
         }
         if (kgrp && HAS_INV) {
+            if (G::SPLIT) { // psi is waited for by the dipolar group otherwise
+                cp_async_wait<0>();
+                group_sync<BK, NK>();
+            }
             KY::run(PP, (const C *)tw.ky.tw, (const C *)tw.ky.lo, tk);
             ZI::run_to_regs(PP, zr, (const C *)tw.kz.tw, (const C *)tw.kz.lo, tk);
         }
@@ -449,8 +513,8 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                 ZF::run(PP, (const C *)tw.kz.tw, (const C *)tw.kz.lo, tk);
             else
                 ZF::run_from_regs(PP, zr, (const C *)tw.kz.tw, (const C *)tw.kz.lo, tk);
-            KYF::run(PP, (const C *)tw.ky.tw, (const C *)tw.ky.lo, tk);
-            plane_out<R, NY, NZ, PS, NK>(P_o, PP, tk);
+            KYF::run_emit(
+                PP, [&](int b, int r, C v) { P_o[r * NZ + b] = v; }, (const C *)tw.ky.tw, (const C *)tw.ky.lo, tk);
         }
     } else {
         using DW = DipolarPlane<R, NY, NZ, NT, 0>;
@@ -470,7 +534,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                 FP[r * FS + k] = wat * (p.x * p.x + p.y * p.y);
             }
         } else {
-            DW::inverse(SP, DP, FP, phi_g, V_g, cdd, tw, tid);
+            DW::template inverse<true>(SP, DP, FP, phi_g, cdd, tw, tid);
             __syncthreads(); // FP complete
             const StepCoef cf = a.step.coef[0];
             const R g3w = (R)cf.g3w, gw15 = (R)cf.gw15;
