@@ -193,6 +193,33 @@ struct PlanePass {
     }
 };
 
+// Stages [S, SE) of in-place pass P on pbuf run jointly with stages [T, TE)
+// of pass Q on qbuf: stage S+k of P and T+k of Q read together, share the
+// barrier, write together.  Two independent butterflies per thread and half
+// the barriers of running the passes one after the other.
+template <class P, int S, int SE, class Q, int T, int TE, class C>
+__device__ __forceinline__ void joint_stages(C *pbuf, const C *ptw, const C *ptl, C *qbuf, const C *qtw,
+                                             const C *qtl, int tid) {
+    constexpr bool DP = S < SE, DQ = T < TE;
+    if constexpr (DP || DQ) {
+        using SP_ = typename P::template Stage<DP ? S : 0>;
+        using SQ_ = typename Q::template Stage<DQ ? T : 0>;
+        typename SP_::Regs pa;
+        typename SQ_::Regs qa;
+        if constexpr (DP)
+            SP_::read(pbuf, pa, ptw, ptl, tid);
+        if constexpr (DQ)
+            SQ_::read(qbuf, qa, qtw, qtl, tid);
+        __syncthreads();
+        if constexpr (DP)
+            SP_::write(pbuf, pa, tid);
+        if constexpr (DQ)
+            SQ_::write(qbuf, qa, tid);
+        __syncthreads();
+        joint_stages<P, S + 1, SE, Q, T + 1, TE>(pbuf, ptw, ptl, qbuf, qtw, qtl, tid);
+    }
+}
+
 struct YZTwid {
     Twid ky, kz, dy, dz;
 };
@@ -280,17 +307,6 @@ template <class R, int NY, int NZ> struct YZShape {
     static constexpr size_t SMEM = SP_B + PP_B + FP_B + DP_B;
     static constexpr int NT0     = 2 * NY * NZ / 16;
     static constexpr int NT      = NT0 < 128 ? 128 : (NT0 > 512 ? 512 : (NT0 + 31) / 32 * 32);
-    // Real time, SPLIT: the first ND threads run the dipolar chain while the
-    // other NK run the kinetic one (named barriers 1 and 2), meeting for phi
-    // and rho.  Measured slower at 128 x 128 x 32 (each chain then runs on half
-    // the warps), so every thread runs both chains one after the other.
-    static constexpr bool SPLIT  = false;
-    static constexpr int ND0     = (NT * 5 / 8 + 31) / 32 * 32;
-    static constexpr int ND      = !SPLIT ? NT : (ND0 > NT - 32 ? NT - 32 : ND0);
-    static constexpr int KOFF    = SPLIT ? ND : 0;
-    static constexpr int NK      = NT - KOFF;
-    static constexpr int BARD    = SPLIT ? 1 : 0;
-    static constexpr int BARK    = SPLIT ? 2 : 0;
 };
 
 // The dipolar chain of a plane, run by NTG threads of barrier group BAR.
@@ -374,7 +390,6 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     using C                = cplx<R>;
     using G                = YZShape<R, NY, NZ>;
     constexpr int NT       = G::NT;
-    constexpr int ND = G::ND, NK = G::NK;
     constexpr int PS = G::PS, FS = G::FS;
     constexpr bool RT      = MODE <= ZM_RT_EPI;
     constexpr bool HAS_INV = (MODE == ZM_RT_MID || MODE == ZM_RT_EPI || MODE == ZM_IT_MID);
@@ -403,47 +418,90 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     if (MODE != ZM_IT_PRO)
         plane_in_async<R, NY, NZ, FS, NT>(FP, V_g, tid);
     cp_async_commit();
-    if (HAS_INV)
+    if (HAS_INV && !RT)
         cp_async_wait<1>(); // S; psi and V are waited for inside the dipolar inverse
     else
         cp_async_wait<0>();
     __syncthreads();
 
     if constexpr (RT) {
-        // The dipolar chain (threads < ND) and the kinetic chain (threads >=
-        // KOFF) meet twice: for phi before the phase, for rho after it.
-        constexpr int BD = G::BARD, BK = G::BARK, KOFF = G::KOFF;
-        using DW = DipolarPlane<R, NY, NZ, ND, BD>;
-        using KY = PlanePass<+1, R, NY, NZ, 1, PS, NK, true, false, false, false, BK>;
-        using KYF = PlanePass<-1, R, NY, NZ, 1, PS, NK, true, false, false, false, BK>;
-        using ZI = PlanePass<+1, R, NZ, NY, PS, 1, NK, true, false, false, false, BK>;
-        using ZF = PlanePass<-1, R, NZ, NY, PS, 1, NK, true, true, false, false, BK>;
+        // The dipolar and the kinetic transforms run stage by stage side by side
+        // (joint_stages); they meet for phi before the phase and rho after it.
+        constexpr int NP = G::NP, LD = G::LD, TD = G::TD;
+        using DYI = PlanePass<+1, R, 2 * NY, NZ, 1, PS, NT, false, true, false, true>;
+        using KYI = PlanePass<+1, R, NY, NZ, 1, PS, NT, true, false>;
+        using C2R = PlanePass<+1, R, LD, NP, 1, TD, NT, false, true, false, true>;
+        using ZI  = PlanePass<+1, R, NZ, NY, PS, 1, NT, true, false>;
+        using ZF  = PlanePass<-1, R, NZ, NY, PS, 1, NT, true, true>;
+        using R2C = PlanePass<-1, R, LD, NP, 1, TD, NT, false, false, true, false>;
+        using KYF = PlanePass<-1, R, NY, NZ, 1, PS, NT, true, false>;
+        using DYF = PlanePass<-1, R, 2 * NY, NZ, 1, PS, NT, false, false, true, false>;
         static_assert(ZI::Last::RADIX == ZF::First::RADIX && ZI::Last::ROUNDS == ZF::First::ROUNDS &&
                           ZI::Last::ITEMS == ZF::First::ITEMS,
                       "paired z transforms share the register layout");
-        const bool dgrp = tid < ND;   // every thread unless SPLIT
-        const bool kgrp = tid >= KOFF; // every thread unless SPLIT
-        const int tk    = tid - KOFF;
+        static_assert(KYF::NSTG >= 2 && DYF::NSTG >= 2, "y lines of at least two stages");
+        const C *dyt = (const C *)tw.dy.tw, *dyl = (const C *)tw.dy.lo;
+        const C *dzt = (const C *)tw.dz.tw, *dzl = (const C *)tw.dz.lo;
+        const C *kyt = (const C *)tw.ky.tw, *kyl = (const C *)tw.ky.lo;
+        const C *kzt = (const C *)tw.kz.tw, *kzl = (const C *)tw.kz.lo;
+        constexpr bool WRITE_PHI = MODE != ZM_RT_MID; // read only after the last iteration
         typename ZI::Last::Regs zr;
-        if (dgrp) {
-            if (HAS_INV) {
-                // phi is needed in global memory only after the last iteration
-                DW::template inverse<MODE != ZM_RT_MID>(SP, DP, FP, phi_g, cdd, tw, tid);
-            } else {
-                // prologue: phi of the previous calc_fi3d
-                for (int e = tid; e < NY * NZ; e += ND) {
-                    const int r = e / NZ, k = e - r * NZ;
-                    FP[r * FS + k] += cdd * phi_g[e];
+        if (HAS_INV) {
+            // dipolar iFFT_y (lower half kept) || kinetic iFFT_y
+            joint_stages<DYI, 0, DYI::NSTG, KYI, 0, KYI::NSTG>(SP, dyt, dyl, PP, kyt, kyl, tid);
+            // C2R pair lines: z[m] = X_a[m] + i X_b[m] over the full 2nz-point
+            // spectrum (bins 1..nz stored at kz - 1, bin 0 zero, bins > nz by
+            // symmetry); DP shares SP's upper half, which holds nothing now
+            for (int e = tid; e < NP * LD; e += NT) {
+                const int p = e % NP, m = e / NP;
+                C z         = C{(R)0, (R)0};
+                if (m > 0) {
+                    const int mm = m <= NZ ? m : LD - m;
+                    const C xa   = SP[(2 * p) * PS + mm - 1];
+                    const C xb   = SP[(2 * p + 1) * PS + mm - 1];
+                    if (m == NZ)
+                        z = C{xa.x, xb.x}; // self-conjugate bin: real parts only
+                    else if (m < NZ)
+                        z = C{xa.x - xb.y, xa.y + xb.x};
+                    else
+                        z = C{xa.x + xb.y, xb.x - xa.y};
+                }
+                DP[p + m * TD] = z;
+            }
+            __syncthreads();
+            // C2R || kinetic iFFT_z, all stages but the last
+            joint_stages<C2R, 0, C2R::NSTG - 1, ZI, 0, ZI::NSTG - 1>(DP, dzt, dzl, PP, kzt, kzl, tid);
+            {
+                // last C2R stage -> FP = V + cdd phi; last iFFT_z stage -> registers
+                typename C2R::Last::Regs ca;
+                C2R::Last::read(DP, ca, dzt, dzl, tid);
+                ZI::Last::read(PP, zr, kzt, kzl, tid);
+#pragma unroll
+                for (int rd = 0; rd < C2R::Last::ROUNDS; ++rd) {
+                    if (!C2R::Last::valid(rd * NT + tid))
+                        break;
+                    const int p = C2R::Last::line(tid, rd);
+#pragma unroll
+                    for (int q = 0; q < C2R::Last::RADIX; ++q) {
+                        if (2 * q >= C2R::Last::RADIX) // pruned: z >= nz is not kept
+                            continue;
+                        const int k = C2R::Last::elem(tid, rd, q);
+                        const C v   = ca[rd][q];
+                        FP[(2 * p) * FS + k] += cdd * v.x;
+                        FP[(2 * p + 1) * FS + k] += cdd * v.y;
+                        if (WRITE_PHI) {
+                            phi_g[(2 * p) * NZ + k]     = v.x;
+                            phi_g[(2 * p + 1) * NZ + k] = v.y;
+                        }
+                    }
                 }
             }
-        }
-        if (kgrp && HAS_INV) {
-            if (G::SPLIT) { // psi is waited for by the dipolar group otherwise
-                cp_async_wait<0>();
-                group_sync<BK, NK>();
+        } else {
+            // prologue: phi of the previous calc_fi3d
+            for (int e = tid; e < NY * NZ; e += NT) {
+                const int r = e / NZ, k = e - r * NZ;
+                FP[r * FS + k] += cdd * phi_g[e];
             }
-            KY::run(PP, (const C *)tw.ky.tw, (const C *)tw.ky.lo, tk);
-            ZI::run_to_regs(PP, zr, (const C *)tw.kz.tw, (const C *)tw.kz.lo, tk);
         }
         __syncthreads(); // FP = V + cdd phi
 
@@ -479,42 +537,101 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
             return p;
         };
         if (MODE == ZM_RT_PRO) {
-            // psi is in real space: every thread takes part in the phase
+            // psi is in real space
             for (int e = tid; e < NY * NZ; e += NT) {
                 const int r = e / NZ, k = e - r * NZ;
                 PP[r * PS + k] = phase(PP[r * PS + k], r, k);
             }
-        } else if (kgrp) {
+        } else {
 #pragma unroll
             for (int rd = 0; rd < ZI::Last::ROUNDS; ++rd) {
-                if (!ZI::Last::valid(rd * NK + tk))
+                if (!ZI::Last::valid(rd * NT + tid))
                     break;
-                const int y = ZI::Last::line(tk, rd);
+                const int y = ZI::Last::line(tid, rd);
 #pragma unroll
                 for (int q = 0; q < ZI::Last::RADIX; ++q)
-                    zr[rd][q] = phase(zr[rd][q], y, ZI::Last::elem(tk, rd, q));
+                    zr[rd][q] = phase(zr[rd][q], y, ZI::Last::elem(tid, rd, q));
             }
             if (MODE == ZM_RT_EPI) {
-                // psi in real space -> global
-                group_sync<BK, NK>();
-                ZI::Last::write(PP, zr, tk);
-                group_sync<BK, NK>();
-                plane_out<R, NY, NZ, PS, NK>(P_o, PP, tk);
+                // psi in real space -> global (the last z reads of PP are behind a barrier)
+                ZI::Last::write(PP, zr, tid);
+                __syncthreads();
+                plane_out<R, NY, NZ, PS, NT>(P_o, PP, tid);
+                return;
             }
         }
-        if (MODE == ZM_RT_EPI)
-            return;
         __syncthreads(); // rho complete
 
-        if (dgrp)
-            DW::forward(SP, DP, FP, S_g, tw, tid);
-        if (kgrp) {
-            if (MODE == ZM_RT_PRO)
-                ZF::run(PP, (const C *)tw.kz.tw, (const C *)tw.kz.lo, tk);
-            else
-                ZF::run_from_regs(PP, zr, (const C *)tw.kz.tw, (const C *)tw.kz.lo, tk);
-            KYF::run_emit(
-                PP, [&](int b, int r, C v) { P_o[r * NZ + b] = v; }, (const C *)tw.ky.tw, (const C *)tw.ky.lo, tk);
+        // R2C pair lines from rho (upper half zero) || kinetic FFT_z
+        for (int e = tid; e < NP * NZ; e += NT) {
+            const int p = e % NP, m = e / NP;
+            DP[p + m * TD] = C{FP[(2 * p) * FS + m], FP[(2 * p + 1) * FS + m]};
+        }
+        if (MODE == ZM_RT_PRO) {
+            __syncthreads();
+            joint_stages<R2C, 0, R2C::NSTG, ZF, 0, ZF::NSTG>(DP, dzt, dzl, PP, kzt, kzl, tid);
+        } else {
+            // first FFT_z stage from the registers (the iFFT_z reads of PP are
+            // behind the two barriers above)
+#pragma unroll
+            for (int rd = 0; rd < ZF::First::ROUNDS; ++rd) {
+                if (!ZF::First::valid(rd * NT + tid))
+                    break;
+                DFT<ZF::First::RADIX, -1, R, true>::run(zr[rd]);
+            }
+            ZF::First::write(PP, zr, tid);
+            __syncthreads();
+            joint_stages<R2C, 0, R2C::NSTG, ZF, 1, ZF::NSTG>(DP, dzt, dzl, PP, kzt, kzl, tid);
+        }
+        // R2C unpacking -> SP rows < ny || kinetic FFT_y stage 0
+        {
+            using K0 = typename KYF::template Stage<0>;
+            typename K0::Regs ka;
+            K0::read(PP, ka, kyt, kyl, tid);
+            for (int e = tid; e < NY * NZ; e += NT) {
+                const int r = e / NZ, m = e - r * NZ + 1; // bins 1..nz
+                const int p = r >> 1;
+                const C zm  = DP[p + m * TD];
+                const C zc  = DP[p + (LD - m) * TD];
+                C x;
+                if ((r & 1) == 0)
+                    x = C{(R)0.5 * (zm.x + zc.x), (R)0.5 * (zm.y - zc.y)}; // (Z_m + conj(Z_{L-m}))/2
+                else
+                    x = C{(R)0.5 * (zm.y + zc.y), (R)0.5 * (zc.x - zm.x)}; // (Z_m - conj(Z_{L-m}))/(2i)
+                SP[r * PS + m - 1] = x;
+            }
+            __syncthreads();
+            K0::write(PP, ka, tid);
+            __syncthreads();
+        }
+        // dipolar FFT_y (upper half zero) || kinetic FFT_y, the last stages
+        // storing straight to global memory
+        joint_stages<DYF, 0, DYF::NSTG - 1, KYF, 1, KYF::NSTG - 1>(SP, dyt, dyl, PP, kyt, kyl, tid);
+        {
+            typename DYF::Last::Regs da;
+            DYF::Last::read(SP, da, dyt, dyl, tid);
+#pragma unroll
+            for (int rd = 0; rd < DYF::Last::ROUNDS; ++rd) {
+                if (!DYF::Last::valid(rd * NT + tid))
+                    break;
+                const int b = DYF::Last::line(tid, rd);
+#pragma unroll
+                for (int q = 0; q < DYF::Last::RADIX; ++q)
+                    S_g[DYF::Last::elem(tid, rd, q) * NZ + b] = da[rd][q];
+            }
+        }
+        {
+            typename KYF::Last::Regs kb;
+            KYF::Last::read(PP, kb, kyt, kyl, tid);
+#pragma unroll
+            for (int rd = 0; rd < KYF::Last::ROUNDS; ++rd) {
+                if (!KYF::Last::valid(rd * NT + tid))
+                    break;
+                const int b = KYF::Last::line(tid, rd);
+#pragma unroll
+                for (int q = 0; q < KYF::Last::RADIX; ++q)
+                    P_o[KYF::Last::elem(tid, rd, q) * NZ + b] = kb[rd][q];
+            }
         }
     } else {
         using DW = DipolarPlane<R, NY, NZ, NT, 0>;
