@@ -528,8 +528,9 @@ template <class R> class Solver final : public SolverBase {
                     b = 2 * S2h + (double)sizeof(R) * (nx + 1) * (ny + 1) * nz; // + the V_dd table
                 } else if (which == GPE_K_F_YZ) {
                     f_yz<ZM_RT_MID>(cur, psi.p, psi.p, coef_dev.p, 0);
-                    // psi R+W, spectrum (2ny rows) R+W, V read, phi write
-                    b = 2 * F + 2 * S2b + Rb + Rb;
+                    // psi R+W, spectrum (2ny rows) R+W, V read (phi is written
+                    // only by the last iteration of a call)
+                    b = 2 * F + 2 * S2b + Rb;
                 } else if (which == GPE_K_F_X) {
                     f_x(cur, true, nullptr);
                     b = 2 * F + 2 * S2h; // kinetic R+W; dipolar reads and writes nx of 2nx planes
