@@ -7,12 +7,15 @@ mirror of the reference's solver interface.
 """
 from .capi import GpeError  # noqa: F401
 from .params import PhysicalParameters, initial_psi, load_params, params_from_json, potential  # noqa: F401
-from .solver import B200GrossPitaevskiSolver, BECEnergies, make_gpe_params  # noqa: F401
+from .batch import B200Batch  # noqa: F401
+from .solver import B200GrossPitaevskiSolver, BECEnergies, make_gpe_params, make_init_params  # noqa: F401
 
 __all__ = [
     "GpeError",
     "PhysicalParameters",
     "B200GrossPitaevskiSolver",
+    "B200Batch",
+    "make_init_params",
     "BECEnergies",
     "initial_psi",
     "potential",

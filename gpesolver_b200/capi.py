@@ -54,6 +54,21 @@ GPE_SCHED_AUTO = 0
 GPE_SCHED_SPLIT = 1
 
 
+class gpe_init_params(ctypes.Structure):
+    _fields_ = [
+        ("omega_x", ctypes.c_double), ("omega_y", ctypes.c_double), ("omega_z", ctypes.c_double),
+        ("aa", ctypes.c_double), ("b", ctypes.c_double), ("dd", ctypes.c_double),
+        ("n_gauss_max", ctypes.c_int),
+        ("bec_droplets_x", ctypes.c_int), ("bec_droplets_y", ctypes.c_int), ("bec_droplets_z", ctypes.c_int),
+    ]
+
+
+# GPE_POT_* (registration order of the reference's potentials) and GPE_INIT_*.
+POTENTIAL_IDS = {"HARMONIC": 0, "MEXICAN": 1, "MEXICAN_FREE": 2, "CYLINDRICAL": 3, "FREE": 4,
+                 "MEXICAN_ASYMETRIC": 5, "MEXICAN_ASYMETRIC_FREE": 6}
+INIT_IDS = {"COS": 0, "GAUSS": 1, "MULTIPLE_GAUSS": 2, "SETUP_GAUSS": 3}
+
+
 _dp = ctypes.POINTER(ctypes.c_double)
 _lib = None
 
@@ -87,6 +102,15 @@ SIGNATURES = [
     ("gpe_launch_count", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     ("gpe_time_kernel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]),
     ("gpe_kernel_name", ctypes.c_char_p, [ctypes.c_int]),
+    ("gpe_init_potential", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(gpe_init_params)]),
+    ("gpe_init_psi", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(gpe_init_params)]),
+    ("gpe_export_potential", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
+    ("gpe_batch_create", ctypes.c_int,
+     [ctypes.POINTER(gpe_params), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("gpe_batch_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpe_batch_member", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("gpe_batch_set_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("gpe_batch_imag_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
     ("gpe_calc_fi3d_noalloc", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
       ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),

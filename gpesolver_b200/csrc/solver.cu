@@ -7,6 +7,7 @@
 // exported fields).
 #include "../../include/gpe_b200.h"
 #include "fused_yz.cuh"
+#include "init.cuh"
 #include "kernels.cuh"
 #include "plan.hpp"
 
@@ -130,6 +131,20 @@ class SolverBase {
     virtual long long launches() const                       = 0;
     virtual void time_kernel(int which, int reps, double *ms, double *bytes) = 0;
     virtual size_t n() const                                 = 0;
+    // device-side initial state and potential (same semantics as load_psi /
+    // load_potential of the host-computed arrays)
+    virtual void init_potential(const PotCoef &c)            = 0;
+    virtual void init_psi(const PsiCoef &c)                  = 0;
+    virtual void export_potential(double *out)               = 0;
+    // batched imaginary time (gpe_batch): the solver's fused IT graph pieces
+    // captured as one branch of a batch graph
+    virtual bool batchable() const                           = 0;
+    virtual void it_batch_begin()                            = 0;
+    virtual long long capture_it_branch(int kind, int count, cudaEvent_t fork, cudaStream_t root) = 0;
+    virtual void it_batch_after(int kind, int count, long long nodes) = 0;
+    virtual void it_batch_end()                              = 0;
+    virtual const void *psi_ptr() const                      = 0;
+    virtual int device() const                               = 0;
 };
 
 // update_edd (src/parameters/parameters.cpp:53-59), FP64, same expression order.
@@ -240,6 +255,11 @@ template <class R> class Solver final : public SolverBase {
     // ---- data in / out ----------------------------------------------------
     void load_psi(const double *h) override {
         GPE_CUDA(cudaMemcpyAsync(staging.p, h, sizeof(double) * 2 * N, cudaMemcpyHostToDevice, cur));
+        load_psi_staged();
+    }
+
+    // load_buffer of the complex128 values in `staging`
+    void load_psi_staged() {
         launch(k_from_f64<R>, grid_elem(2 * N), 256, 0, cur, (const double *)staging.p,
                reinterpret_cast<R *>(psi.p), 2 * N);
         GPE_CUDA(cudaMemcpyAsync(psii.p, psi.p, sizeof(C) * N, cudaMemcpyDeviceToDevice, cur));
@@ -265,6 +285,56 @@ template <class R> class Solver final : public SolverBase {
         GPE_CUDA(cudaMemcpyAsync(staging.p, h, sizeof(double) * N, cudaMemcpyHostToDevice, cur));
         launch(k_from_f64<R>, grid_elem(N), 256, 0, cur, (const double *)staging.p, V.p, N);
         GPE_CUDA(cudaStreamSynchronize(cur));
+    }
+
+    InitGeom geom() const { return InitGeom{nx, ny, nz, P.dx, P.dy, P.dz}; }
+
+    void init_potential(const PotCoef &c) override {
+        launch(k_init_potential, grid_elem(N), 256, 0, cur, staging.p, geom(), c);
+        launch(k_from_f64<R>, grid_elem(N), 256, 0, cur, (const double *)staging.p, V.p, N);
+        GPE_CUDA(cudaStreamSynchronize(cur));
+    }
+
+    void init_psi(const PsiCoef &c) override {
+        launch(k_init_psi, grid_elem(N), 256, 0, cur, staging.p, geom(), c);
+        load_psi_staged();
+    }
+
+    void export_potential(double *h) override {
+        launch(k_to_f64<R>, grid_elem(N), 256, 0, cur, (const R *)V.p, staging.p, N,
+               (const double *)one_ptr(), 1);
+        GPE_CUDA(cudaMemcpyAsync(h, staging.p, sizeof(double) * N, cudaMemcpyDeviceToHost, cur));
+        GPE_CUDA(cudaStreamSynchronize(cur));
+    }
+
+    // ---- batched imaginary time ----------------------------------------------
+    bool batchable() const override { return fused; }
+    const void *psi_ptr() const override { return psi.p; }
+    int device() const override { return P.device; }
+    void it_batch_begin() override {
+        if (!lazy)
+            set_divisor_one();
+    }
+    // Records this solver's fused IT graph piece (kind 20: prologue, 21: `count`
+    // iterations) on its capture stream as a branch from `fork` that joins `root`.
+    long long capture_it_branch(int kind, int count, cudaEvent_t fork, cudaStream_t root) override {
+        const long long before = n_launch;
+        GPE_CUDA(cudaStreamWaitEvent(cap_stream, fork, 0));
+        capture_fused(kind, count);
+        GPE_CUDA(cudaEventRecord(ev_join, cap_stream));
+        GPE_CUDA(cudaStreamWaitEvent(root, ev_join, 0));
+        const long long nodes = n_launch - before;
+        n_launch              = before;
+        return nodes;
+    }
+    void it_batch_after(int kind, int count, long long nodes) override {
+        n_launch += nodes;
+        if (kind == 21 && (count & 1))
+            std::swap(psi.p, psii.p);
+    }
+    void it_batch_end() override {
+        lazy = true;
+        check_status();
     }
 
     void export_psi(double *h) override {
@@ -1227,6 +1297,7 @@ template <class R> class Solver final : public SolverBase {
 struct gpe_handle {
     std::unique_ptr<gpe::SolverBase> impl;
     int device = 0;
+    gpe_params params{};
 };
 
 namespace {
@@ -1299,11 +1370,262 @@ int gpe_create(const gpe_params *p, gpe_handle **out) {
     return guarded([&] {
         auto h    = std::make_unique<gpe_handle>();
         h->device = p->device;
+        h->params = *p;
         if (p->precision == GPE_PREC_C64)
             h->impl.reset(new gpe::Solver<float>(*p));
         else
             h->impl.reset(new gpe::Solver<double>(*p));
         *out = h.release();
+    });
+}
+
+} // extern "C"
+
+using gpe::Error; // for GPE_CUDA outside namespace gpe
+
+struct gpe_batch {
+    std::vector<gpe_handle *> members;
+    int device          = 0;
+    cudaStream_t own    = nullptr; // the batch's own stream
+    cudaStream_t cur    = nullptr;
+    cudaStream_t root   = nullptr; // capture origin
+    cudaEvent_t fork    = nullptr;
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<long long> nodes; // kernel launches per member
+    };
+    std::map<std::tuple<int, int, std::vector<const void *>>, Graph> graphs;
+
+    ~gpe_batch() {
+        cudaSetDevice(device);
+        if (cur)
+            cudaStreamSynchronize(cur);
+        for (auto &kv : graphs)
+            cudaGraphExecDestroy(kv.second.exec);
+        for (auto *m : members)
+            delete m;
+        if (fork)
+            cudaEventDestroy(fork);
+        if (root)
+            cudaStreamDestroy(root);
+        if (own)
+            cudaStreamDestroy(own);
+    }
+
+    // One launch of the batch graph for (kind, count): kind 20 the IT prologue,
+    // 21 `count` IT iterations of every member.
+    void run(int kind, int count) {
+        std::vector<const void *> sig;
+        for (auto *m : members)
+            sig.push_back(m->impl->psi_ptr());
+        auto key = std::make_tuple(kind, count, sig);
+        auto it  = graphs.find(key);
+        if (it == graphs.end()) {
+            Graph g;
+            GPE_CUDA(cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal));
+            try {
+                GPE_CUDA(cudaEventRecord(fork, root));
+                for (auto *m : members)
+                    g.nodes.push_back(m->impl->capture_it_branch(kind, count, fork, root));
+            } catch (...) {
+                cudaGraph_t gr = nullptr;
+                cudaStreamEndCapture(root, &gr);
+                if (gr)
+                    cudaGraphDestroy(gr);
+                throw;
+            }
+            cudaGraph_t gr;
+            GPE_CUDA(cudaStreamEndCapture(root, &gr));
+            GPE_CUDA(cudaGraphInstantiate(&g.exec, gr, 0));
+            cudaGraphDestroy(gr);
+            it = graphs.emplace(key, std::move(g)).first;
+        }
+        GPE_CUDA(cudaGraphLaunch(it->second.exec, cur));
+        for (size_t m = 0; m < members.size(); ++m)
+            members[m]->impl->it_batch_after(kind, count, it->second.nodes[m]);
+    }
+};
+
+namespace {
+
+// PsiCoef of DataInitializer::init_with_* (initializer.cpp:46-219), host FP64
+// with the reference's expressions.
+gpe::PsiCoef psi_coef(const gpe_params &p, int strategy, const gpe_init_params &ip) {
+    gpe::PsiCoef c{};
+    c.strategy = strategy;
+    if (strategy == GPE_INIT_COS) {
+        c.rrr = (static_cast<int>(p.nx / 2) * p.dx);
+        c.dd  = ip.dd;
+    } else if (strategy == GPE_INIT_GAUSS) {
+        c.sx = (p.nx * p.dx) / 10.;
+        c.sy = (p.ny * p.dy) / 10.;
+        c.sz = (p.nz * p.dz) / 10.;
+    } else if (strategy == GPE_INIT_MULTIPLE_GAUSS) {
+        c.sx = (p.nx * p.dx) / 20.;
+        c.sy = (p.ny * p.dy) / 20.;
+        c.sz = (p.nz * p.dz) / 20.;
+        const int n = ip.n_gauss_max;
+        if (n < 0 || n > gpe::kMaxGaussCentres)
+            throw gpe::Error(GPE_ERR_ARG, "n_gauss_max must be in 0..64");
+        c.ncent = n;
+        const double y0 = (0 - (static_cast<int>(p.ny / 2))) * p.dy;
+        for (int idx = 0; idx < n; ++idx) {
+            c.cx[idx] = idx % 2 ? ip.dd : -ip.dd;
+            if (n % 2 == 1) {
+                const int center_y_idx = n / 2;
+                c.cy[idx]              = (idx - center_y_idx) * (p.ny * p.dy) / 2. / (n + 1.);
+            } else {
+                const int y_idx = (idx / 2 + 1), y_maximas = (n / 2 + 1);
+                c.cy[idx]       = y0 + y_idx * (p.ny * p.dy) / y_maximas;
+            }
+        }
+    } else if (strategy == GPE_INIT_SETUP_GAUSS) {
+        c.sx = (p.nx * p.dx) / 20.;
+        c.sy = (p.ny * p.dy) / 20.;
+        c.sz = (p.nz * p.dz) / 20.;
+        const int bx = ip.bec_droplets_x, by = ip.bec_droplets_y, bz = ip.bec_droplets_z;
+        if (bx < 0 || by < 0 || bz < 0 || (long)bx * by * bz > gpe::kMaxGaussCentres)
+            throw gpe::Error(GPE_ERR_ARG, "bec_droplets_x * _y * _z must be in 0..64");
+        c.ncent = bx * by * bz;
+        c.zcent = 1;
+        const double x_tot = p.nx * p.dx, y_tot = p.ny * p.dy, z_tot = p.nz * p.dz;
+        for (int i = 0; i < bx; ++i)
+            for (int j = 0; j < by; ++j)
+                for (int k = 0; k < bz; ++k) {
+                    const int idx          = i * by * bz + j * bz + k;
+                    const double spacing_x = x_tot / static_cast<double>(bx + 1);
+                    const double spacing_y = y_tot / static_cast<double>(by + 1);
+                    const double spacing_z = z_tot / static_cast<double>(bz + 1);
+                    c.cx[idx]              = -x_tot / 2 + spacing_x * (i + 1);
+                    c.cy[idx]              = -y_tot / 2 + spacing_y * (j + 1);
+                    c.cz[idx]              = -z_tot / 2 + spacing_z * (k + 1);
+                }
+    } else {
+        throw gpe::Error(GPE_ERR_ARG, "unknown initial-state strategy");
+    }
+    return c;
+}
+
+} // namespace
+
+extern "C" {
+
+int gpe_init_potential(gpe_handle *h, int pote, const gpe_init_params *ip) {
+    GPE_HANDLE(h);
+    if (!ip)
+        return bad("null init params");
+    if (pote < 0 || pote >= gpe::POT_COUNT)
+        return bad("unknown potential");
+    return guarded([&] {
+        const gpe_params &p = h->params;
+        gpe::PotCoef c{};
+        c.key = pote;
+        c.m   = p.m;
+        c.wx = ip->omega_x, c.wy = ip->omega_y, c.wz = ip->omega_z;
+        c.aa = ip->aa, c.b = ip->b;
+        if (pote == GPE_POT_MEXICAN_ASYMETRIC || pote == GPE_POT_MEXICAN_ASYMETRIC_FREE) {
+            // potentials.hpp:133-137
+            const double conv = 27211.4 * 11.6 * 1e9;
+            const double nK25 = 0.25 / conv;
+            c.slope           = nK25 / ip->dd;
+        }
+        h->impl->init_potential(c);
+    });
+}
+
+int gpe_init_psi(gpe_handle *h, int strategy, const gpe_init_params *ip) {
+    GPE_HANDLE(h);
+    if (!ip)
+        return bad("null init params");
+    return guarded([&] { h->impl->init_psi(psi_coef(h->params, strategy, *ip)); });
+}
+
+int gpe_export_potential(gpe_handle *h, double *V, size_t n) {
+    GPE_HANDLE(h);
+    if (!V || n != h->impl->n())
+        return bad("potential buffer size mismatch");
+    return guarded([&] { h->impl->export_potential(V); });
+}
+
+int gpe_batch_create(const gpe_params *members, int count, gpe_batch **out) {
+    if (!members || !out || count <= 0)
+        return bad("null argument or empty batch");
+    *out = nullptr;
+    for (int m = 0; m < count; ++m)
+        if (members[m].device != members[0].device)
+            return bad("batch members must share one device");
+    return guarded([&] {
+        auto b    = std::make_unique<gpe_batch>();
+        b->device = members[0].device;
+        GPE_CUDA(cudaSetDevice(b->device));
+        GPE_CUDA(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking));
+        GPE_CUDA(cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking));
+        GPE_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        b->cur = b->own;
+        for (int m = 0; m < count; ++m) {
+            gpe_handle *h = nullptr;
+            const int rc  = gpe_create(&members[m], &h);
+            if (rc != GPE_OK)
+                throw gpe::Error(rc, "batch member " + std::to_string(m) + ": " + gpe::last_error());
+            b->members.push_back(h);
+            if (!h->impl->batchable())
+                throw gpe::Error(GPE_ERR_STATE, "batch member " + std::to_string(m) +
+                                                    ": needs complex64 and a grid with the fused pipeline");
+            h->impl->set_stream(b->cur);
+        }
+        *out = b.release();
+    });
+}
+
+int gpe_batch_destroy(gpe_batch *b) {
+    delete b;
+    return GPE_OK;
+}
+
+int gpe_batch_member(gpe_batch *b, int m, gpe_handle **h) {
+    if (!b || !h || m < 0 || m >= (int)b->members.size())
+        return bad("bad batch or member index");
+    *h = b->members[m];
+    return GPE_OK;
+}
+
+int gpe_batch_set_stream(gpe_batch *b, void *s) {
+    if (!b)
+        return bad("null batch");
+    if (cudaSetDevice(b->device) != cudaSuccess)
+        return bad("cudaSetDevice failed");
+    return guarded([&] {
+        b->cur = s ? (cudaStream_t)s : b->own;
+        for (auto *m : b->members)
+            m->impl->set_stream(b->cur);
+    });
+}
+
+int gpe_batch_imag_steps(gpe_batch *b, long k) {
+    if (!b)
+        return bad("null batch");
+    if (k < 0)
+        return bad("negative iteration count");
+    if (cudaSetDevice(b->device) != cudaSuccess)
+        return bad("cudaSetDevice failed");
+    if (k == 0)
+        return GPE_OK;
+    return guarded([&] {
+        for (auto *m : b->members)
+            m->impl->it_batch_begin();
+        // the fused imaginary-time schedule of every member (fused_imag):
+        // prologue, chunks of 64 iterations, remainder
+        b->run(20, 0);
+        constexpr int CH = 64;
+        long done        = 0;
+        while (k - done >= CH) {
+            b->run(21, CH);
+            done += CH;
+        }
+        if (k - done > 0)
+            b->run(21, (int)(k - done));
+        for (auto *m : b->members)
+            m->impl->it_batch_end();
     });
 }
 

@@ -259,16 +259,20 @@ def load_params(path: str = "gpe_params.json") -> PhysicalParameters:
 # Potentials and initial states (DataInitializer, host FP64)
 # ---------------------------------------------------------------------------
 def _pote_eval(p: PhysicalParameters, key: str, x, y, z):
-    """PotentialRegistry lambdas (src/parameters/potentials.hpp:76-157)."""
+    """PotentialRegistry lambdas (src/parameters/potentials.hpp:76-157).
+
+    std::pow(x, 4) of an integer x is the correctly rounded x^4, which is
+    (x*x)*(x*x) (x*x is exact); numpy's power is off by an ulp on some x."""
     m = p.m
+    x4 = (x * x) * (x * x)
     if key == "HARMONIC":
         return (0.5 * m * x ** 2 * p.omega_x ** 2 + 0.5 * m * y ** 2 * p.omega_y ** 2) + \
             0.5 * m * z ** 2 * p.omega_z ** 2
     if key == "MEXICAN":
-        vx = -p.b * x ** 2 + p.aa * np.power(x, 4)
+        vx = -p.b * x ** 2 + p.aa * x4
         return (vx + 0.5 * m * y ** 2 * p.omega_y ** 2) + 0.5 * m * z ** 2 * p.omega_z ** 2
     if key == "MEXICAN_FREE":
-        vx = p.aa * np.power(x, 4)
+        vx = p.aa * x4
         return (vx + 0.5 * m * y ** 2 * p.omega_y ** 2) + 0.5 * m * z ** 2 * p.omega_z ** 2
     if key == "CYLINDRICAL":
         r = np.sqrt(x * x + y * y)
@@ -280,9 +284,9 @@ def _pote_eval(p: PhysicalParameters, key: str, x, y, z):
         conv = 27211.4 * 11.6 * 1e9
         slope = (0.25 / conv) / p.dd
         if key == "MEXICAN_ASYMETRIC":
-            vx = -p.b * x ** 2 + p.aa * np.power(x, 4) - slope * x
+            vx = -p.b * x ** 2 + p.aa * x4 - slope * x
         else:
-            vx = p.aa * np.power(x, 4) - slope * x
+            vx = p.aa * x4 - slope * x
         return (vx + 0.5 * m * y ** 2 * p.omega_y ** 2) + 0.5 * m * z ** 2 * p.omega_z ** 2
     raise ParamsError("Not know potential option: " + key)
 

@@ -47,7 +47,33 @@ def make_gpe_params(p: PhysicalParameters, precision: str = "c64", device: int =
     return g
 
 
+def make_init_params(p: PhysicalParameters) -> capi.gpe_init_params:
+    """gpe_init_params: the fields the potentials and initialisers read."""
+    g = capi.gpe_init_params()
+    g.omega_x, g.omega_y, g.omega_z = p.omega_x, p.omega_y, p.omega_z
+    g.aa, g.b, g.dd = p.aa, p.b, p.dd
+    g.n_gauss_max = p.n_gauss_max
+    g.bec_droplets_x, g.bec_droplets_y, g.bec_droplets_z = p.bec_droplets_x, p.bec_droplets_y, p.bec_droplets_z
+    return g
+
+
 class B200GrossPitaevskiSolver:
+    @classmethod
+    def _borrow(cls, handle: ctypes.c_void_p, params: PhysicalParameters, precision: str = "c64"):
+        """A view of a handle owned elsewhere (a batch member): close() leaves it alone."""
+        self = cls.__new__(cls)
+        self.params = dataclasses.replace(params)
+        self.precision = precision
+        self._L = capi.lib()
+        self._gp = None
+        self._h = handle
+        self._borrowed = True
+        self.n = params.n
+        self.xnorma = 0.0
+        self.enes = []
+        self.ene = None
+        return self
+
     def __init__(self, params: PhysicalParameters, precision: str = "c64", device: int = 0,
                  schedule: str = "auto"):
         # the solver owns its parameters (real_steps advances edd on this copy,
@@ -66,6 +92,9 @@ class B200GrossPitaevskiSolver:
 
     # -- lifecycle ---------------------------------------------------------
     def close(self) -> None:
+        if getattr(self, "_borrowed", False):
+            self._h = None
+            return
         if getattr(self, "_h", None):
             self._L.gpe_destroy(self._h)
             self._h = None
@@ -112,6 +141,28 @@ class B200GrossPitaevskiSolver:
         if a.size != self.n:
             raise capi.GpeError(capi.GPE_ERR_ARG, "bad potential import")
         capi.check(self._L.gpe_load_potential(self._h, capi.dptr(a), self.n))
+
+    def init_pote(self, key: Optional[str] = None) -> None:
+        """load_pote(init_pote()) with V computed on the device (FP64,
+        bit-identical to the host potential)."""
+        key = key or self.params.pote_key
+        ip = make_init_params(self.params)
+        capi.check(self._L.gpe_init_potential(self._h, capi.POTENTIAL_IDS[key], ctypes.byref(ip)))
+
+    def init_buffer(self, strategy: Optional[str] = None) -> None:
+        """load_buffer(psi_0) with psi_0 computed on the device from the
+        initialisation strategy (COS, GAUSS, MULTIPLE_GAUSS, SETUP_GAUSS)."""
+        strategy = strategy or self.params.init_strategy
+        if strategy not in capi.INIT_IDS:
+            raise capi.GpeError(capi.GPE_ERR_ARG, f"no device initialiser for {strategy}")
+        ip = make_init_params(self.params)
+        capi.check(self._L.gpe_init_psi(self._h, capi.INIT_IDS[strategy], ctypes.byref(ip)))
+
+    def export_pote(self) -> np.ndarray:
+        """The potential the solver holds (buf_data->pote), FP64."""
+        out = np.zeros(self.n)
+        capi.check(self._L.gpe_export_potential(self._h, capi.dptr(out), self.n))
+        return out.reshape(self.params.shape)
 
     def export_data(self) -> np.ndarray:
         """psi as complex128 of shape (nx, ny, nz)."""

@@ -171,6 +171,58 @@ int gpe_time_kernel(gpe_handle *h, int which, int reps, double *ms_per_launch,
 /* Name of kernel `which` as it appears in a profiler's launch list. */
 const char *gpe_kernel_name(int which);
 
+/* --- device-side initial state and potential --- */
+
+/* Potential ids, in the reference's registration order
+ * (src/parameters/potentials.hpp:76-157). */
+enum {
+    GPE_POT_HARMONIC = 0, GPE_POT_MEXICAN, GPE_POT_MEXICAN_FREE, GPE_POT_CYLINDRICAL, GPE_POT_FREE,
+    GPE_POT_MEXICAN_ASYMETRIC, GPE_POT_MEXICAN_ASYMETRIC_FREE
+};
+/* Initial-state strategies computed from formulas (InitializationOption,
+ * src/parameters/complex_param.hpp:57-97; the file-based ones load psi). */
+enum { GPE_INIT_COS = 0, GPE_INIT_GAUSS, GPE_INIT_MULTIPLE_GAUSS, GPE_INIT_SETUP_GAUSS };
+
+/* The PhysicalParameters fields the potentials and initialisers read, in
+ * atomic units (parameters.hpp:10-123, as init_parameters leaves them). */
+typedef struct gpe_init_params {
+    double omega_x, omega_y, omega_z;
+    double aa, b;           /* MEXICAN coefficients (parameters.cpp:38-39) */
+    double dd;              /* double-well distance */
+    int n_gauss_max;        /* MULTIPLE_GAUSS maxima (at most 64) */
+    int bec_droplets_x, bec_droplets_y, bec_droplets_z; /* SETUP_GAUSS (product at most 64) */
+} gpe_init_params;
+
+/* DataInitializer::init_pote + load_pote (src/initializer/initializer.cpp:229-248,
+ * solver.cpp:127-131) computed on the device in FP64: bit-identical to the
+ * reference's host potential. */
+int gpe_init_potential(gpe_handle *h, int pote, const gpe_init_params *ip);
+/* DataInitializer::init_with_* + load_buffer (initializer.cpp:46-219,
+ * solver.cpp:118-125) computed on the device in FP64 (exp / cos within an ulp
+ * or two of the host library), then normalised as load_buffer does. */
+int gpe_init_psi(gpe_handle *h, int strategy, const gpe_init_params *ip);
+/* The potential the handle holds (buf_data->pote), widened to FP64. */
+int gpe_export_potential(gpe_handle *h, double *V, size_t n);
+
+/* --- batched imaginary time (parameter sweeps) --- */
+
+/* A set of independent solves on one GPU whose imaginary-time iterations run
+ * as one CUDA-graph launch per chunk of iterations: every member's kernel chain
+ * is a branch of the same graph, so small grids fill the GPU together.  The
+ * reference runs such sweeps as separate processes, one after the other.
+ * Members may differ in grid and parameters; each must take the fused
+ * complex64 pipeline (compiled grid sizes). */
+typedef struct gpe_batch gpe_batch;
+int gpe_batch_create(const gpe_params *members, int count, gpe_batch **out);
+int gpe_batch_destroy(gpe_batch *b);
+/* The handle of member m (owned by the batch): load, initialise, export and
+ * measure members with the single-handle calls. */
+int gpe_batch_member(gpe_batch *b, int m, gpe_handle **h);
+/* Stream of the batch and of every member (NULL: the batch's own stream). */
+int gpe_batch_set_stream(gpe_batch *b, void *cuda_stream);
+/* k imaginary-time iterations of every member (gpe_imag_steps on each). */
+int gpe_batch_imag_steps(gpe_batch *b, long k);
+
 /* --- allocation-free variant --- */
 
 /* Size of the file-scope device array gpe_calc_fi3d_noalloc works in. */

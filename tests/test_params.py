@@ -5,6 +5,7 @@ The required-key cases mirror the reference's own FileManager tests
 and initial states are compared with the FP64 oracle.
 """
 import copy
+import os
 
 import numpy as np
 import pytest
@@ -145,3 +146,21 @@ def test_update_edd_matches_oracle():
         p.update_edd(it)
         L.gpeo_update_edd(ctypes.byref(op), it)
         assert (p.edd, p.ggp11, p.gamma) == (op.edd, op.ggp11, op.gamma)
+
+
+@pytest.mark.parametrize("key", ["HARMONIC", "MEXICAN", "MEXICAN_FREE", "CYLINDRICAL", "FREE",
+                                 "MEXICAN_ASYMETRIC", "MEXICAN_ASYMETRIC_FREE"])
+@pytest.mark.parametrize("dims", [(64, 48, 24), (128, 128, 32)])
+def test_potential_bit_identical_to_reference_at_full_size(key, dims):
+    """At these grids x^4 exceeds 2^53: the host potential must round it as
+    std::pow does (the reference's own code, compiled, is the comparison)."""
+    if not os.path.exists(O.REF_SO):
+        pytest.skip("reference harness not built")
+    cfg = O.default_config(nx=dims[0], ny=dims[1], nz=dims[2], pote_strategy=key)
+    p = G.params_from_json(as_json(cfg))
+    r = O.RefSolver(cfg, load_initial=False)
+    try:
+        want = r.pote()
+    finally:
+        r.close()
+    np.testing.assert_array_equal(G.potential(p), want)
