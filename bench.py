@@ -434,6 +434,153 @@ def run_profile(iters: int) -> None:
         print(f"profile run: {iters} RT iterations, {s.launch_count()} kernel launches", flush=True)
 
 
+# ---------------------------------------------------------------------------
+# parameter sweep (batched imaginary time)
+# ---------------------------------------------------------------------------
+SWEEP_METRIC = "batched IT sweep member-iterations/s"
+
+
+def reference_it_seconds(grid, budget_s: float) -> tuple[float, int]:
+    """Seconds per imaginary-time iteration of the reference's CPU solver at one
+    sweep grid (CYLINDRICAL, GAUSS), from a bounded sample."""
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    cfg = O.default_config(nx=grid[0], ny=grid[1], nz=grid[2], init_strategy="GAUSS",
+                           pote_strategy="CYLINDRICAL", fftw_n_threads=threads)
+    S = O.RefSolver(cfg) if O.ref_available() else O.OracleSolver(cfg)
+    S.imag_steps(1)
+    n, t0 = 0, time.perf_counter()
+    while n < 2 or (time.perf_counter() - t0 < budget_s and n < 500):
+        S.imag_steps(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    S.close()
+    return dt / n, n
+
+
+def run_sweep(args):
+    """64 imaginary-time ground states with seeded parameters (SplitMix64, seed
+    0) over mixed grids, as one B200Batch, against the same members run one
+    after the other on the GPU and the reference's CPU solver."""
+    import collections
+
+    import numpy as np
+    import torch
+
+    import gpesolver_b200 as G
+    from gpesolver_b200 import sweep
+
+    iters = args.sweep_iters
+    js = sweep.sweep_json(count=args.sweep_members, seed=0, iter_imag=iters)
+    ps = [G.params_from_json(j) for j in js]
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    b = G.B200Batch(ps)
+    b.set_stream(stream.cuda_stream)
+
+    def init_all():
+        for m in b.members:
+            m.init_pote()
+            m.init_buffer()
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, args.warmup - 2)):  # builds the batch graphs
+            init_all()
+            b.imag_steps(iters)
+    stream.synchronize()
+    launches0 = sum(m.launch_count() for m in b.members)
+    times, e2e_times = [], []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                init_all()
+                flush.zero_()
+                e0, e1 = ev(), ev()
+                e0.record(stream)
+                b.imag_steps(iters)
+                e1.record(stream)
+            stream.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+    clocks = clk.summary()
+    launches = (sum(m.launch_count() for m in b.members) - launches0) // args.steps
+    # end to end: device-side initialisation, the solves, psi and energies to the host
+    for _ in range(2):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0, e1 = ev(), ev()
+            e0.record(stream)
+            init_all()
+            b.imag_steps(iters)
+            out = [m.export_data() for m in b.members]
+            en = [m.calc_energy() for m in b.members]
+            e1.record(stream)
+        stream.synchronize()
+        e2e_times.append(e0.elapsed_time(e1) / 1e3)
+    d2h = sum(int(o.size) * 16 for o in out) + 48 * len(out)
+    e_tot = np.array([e.e_total for e in en])
+    b.close()
+
+    # the same members one after the other (each a fused single solve)
+    seq = 0.0
+    for p in ps:
+        with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
+            s.set_stream(stream.cuda_stream)
+            with torch.cuda.stream(stream):
+                s.init_pote()
+                s.init_buffer()
+                s.imag_steps(iters)  # graphs
+                s.init_buffer()
+                flush.zero_()
+                e0, e1 = ev(), ev()
+                e0.record(stream)
+                s.imag_steps(iters)
+                e1.record(stream)
+            stream.synchronize()
+            seq += e0.elapsed_time(e1) / 1e3
+
+    t = statistics.median(times)
+    counts = collections.Counter((j["nx"], j["ny"], j["nz"]) for j in js)
+    cpu = None
+    if not args.no_cpu_baseline:
+        per = {g: reference_it_seconds(g, args.cpu_budget / len(counts)) for g in counts}
+        cpu_sweep_s = sum(counts[g] * per[g][0] * iters for g in counts)
+        cpu = {"value": len(ps) * iters / cpu_sweep_s, "unit": "member-iterations/s",
+               "cores": os.cpu_count() or 1, "kind": "reference",
+               "sample": "; ".join(f"{per[g][1]} IT iterations at {g[0]}x{g[1]}x{g[2]}" for g in counts)
+                         + " (the sweep time is these per-iteration times x members x iterations; "
+                           "FP64 FFTW-API shim, FFTW3 absent)",
+               "sweep_seconds": cpu_sweep_s}
+    line = {
+        "metric": SWEEP_METRIC, "value": len(ps) * iters / t, "unit": "member-iterations/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic (SplitMix64 seed 0 parameters; device-side CYLINDRICAL trap and GAUSS state)",
+        "config": {"workload": f"{len(ps)} imaginary-time solves x {iters} iterations, CYLINDRICAL, "
+                               f"GAUSS, edd~U[1.2,1.8], n_atoms~U[1e4,5e4], omega_r~U[40,80] Hz, "
+                               f"omega_z/omega_r~U[1,4], dx=dy=120 nm, dz=600 nm",
+                   "grids": {f"{g[0]}x{g[1]}x{g[2]}": c for g, c in sorted(counts.items())},
+                   "seed": 0, "generator": "SplitMix64",
+                   "schedule": "one CUDA graph per 64-iteration chunk, one branch per member",
+                   "l2": "flushed before each timed sweep"},
+        "sweep_seconds": t,
+        "sequential_gpu": {"value": len(ps) * iters / seq, "sweep_seconds": seq,
+                           "note": "the same members one after the other, each alone on the GPU"},
+        "e2e": {"value": len(ps) * iters / statistics.median(e2e_times), "unit": "member-iterations/s",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+                "note": "device-side initialisation, the solves, psi and energies of every member to the host"},
+        "gpu_launches": int(launches),
+        "energy_meV_range": [float(e_tot.min() * 27211.386), float(e_tot.max() * 27211.386)],
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -443,6 +590,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="rt", choices=["rt", "sweep"],
+                    help="rt: the headline real-time benchmark; sweep: 64 batched imaginary-time solves")
+    ap.add_argument("--sweep-members", type=int, default=64)
+    ap.add_argument("--sweep-iters", type=int, default=1000)
     ap.add_argument("--profile", type=int, default=0,
                     help="profiling run: set up the workload (10 IT iterations), then run this many "
                          "RT iterations untimed and exit")
@@ -452,7 +603,9 @@ def main():
         return
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
-    if args.impl == "reference":
+    if args.workload == "sweep":
+        run_sweep(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_our_arm(args)

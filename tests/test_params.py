@@ -164,3 +164,20 @@ def test_potential_bit_identical_to_reference_at_full_size(key, dims):
     finally:
         r.close()
     np.testing.assert_array_equal(G.potential(p), want)
+
+
+def test_sweep_generator_is_seeded_splitmix64():
+    from gpesolver_b200 import sweep
+
+    r = sweep.SplitMix64(0)
+    # published first outputs of SplitMix64 from seed 0
+    assert r.next() == 0xE220A8397B1DCDAF
+    assert r.next() == 0x6E789E6AA1B965F4
+    a, b = sweep.sweep_json(count=64, seed=0), sweep.sweep_json(count=64, seed=0)
+    assert a == b and len(a) == 64
+    for j in a:
+        assert (j["nx"], j["ny"], j["nz"]) in sweep.GRIDS
+        assert 1.2 <= j["edd"] < 1.8 and 1e4 <= j["n_atoms"] < 5e4
+        assert 40 <= j["omega_x"] == j["omega_y"] < 80 and 1 <= j["omega_z"] / j["omega_x"] < 4
+    ps = sweep.sweep_params(count=3, seed=1)
+    assert all(p.pote_key == "CYLINDRICAL" and p.init_strategy == "GAUSS" for p in ps)
