@@ -581,6 +581,102 @@ def run_sweep(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# accuracy against FP64 (complex64 path vs the complex128 path)
+# ---------------------------------------------------------------------------
+def run_accuracy(args):
+    """psi relative L2 error, energy error and norm drift of the complex64 path
+    against the FP64 path (complex128, which matches the reference's CPU code to
+    ~1e-12 per call) for the README full simulation and the 256x256x64 ramp
+    study; beside them, how far two FP64 runs whose start differs by 1e-7
+    (relative, seeded noise) drift apart -- the dynamics' own sensitivity."""
+    import numpy as np
+
+    import gpesolver_b200 as G
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    def rel_phase(a, b):
+        """relative L2 after removing a global phase (the chemical potential
+        rotates psi as a whole; a tiny energy offset shows up as a phase)"""
+        a, b = a.reshape(-1), b.reshape(-1)
+        ov = np.vdot(a, b)
+        return rel(a * (ov / abs(ov)), b)
+
+    rng = np.random.default_rng(1)
+
+    def perturbed(psi):
+        x = psi.reshape(-1)
+        return x * (1 + 1e-7 * rng.standard_normal(x.size))
+
+    def track(runs, ref_key, checkpoints, first_iter=0):
+        """Advance every solver in `runs` to each checkpoint; errors vs runs[ref_key]."""
+        rows, done = [], 0
+        n0 = {k: s.calc_norm() for k, s in runs.items()}
+        for c in checkpoints:
+            for s in runs.values():
+                s.real_steps(c - done, first_iter + done)
+            done = c
+            ref_psi = runs[ref_key].export_data()
+            ref_e = runs[ref_key].calc_energy().e_total
+            row = {"rt_iterations": c}
+            for k, s in runs.items():
+                if k == ref_key:
+                    row[f"{k}_norm_drift"] = s.calc_norm() / n0[k] - 1
+                    continue
+                psi = s.export_data()
+                row[f"{k}_psi_rel_l2"] = rel(psi, ref_psi)
+                row[f"{k}_psi_rel_l2_phase_aligned"] = rel_phase(psi, ref_psi)
+                row[f"{k}_energy_rel"] = abs(s.calc_energy().e_total - ref_e) / abs(ref_e)
+                row[f"{k}_norm_drift"] = s.calc_norm() / n0[k] - 1
+            rows.append(row)
+        return rows
+
+    out = {}
+    # README full simulation at 128x128x32: 1000 IT, switch to MEXICAN_FREE, 10000 RT
+    p = G.params_from_json(workload_json())
+    c64 = G.B200GrossPitaevskiSolver(p, precision="c64")
+    c128 = G.B200GrossPitaevskiSolver(p, precision="c128")
+    for s in (c64, c128):
+        s.init_pote()
+        s.init_buffer()
+        s.imag_steps(1000)
+    it_row = {"psi_rel_l2": rel(c64.export_data(), c128.export_data()),
+              "energy_rel": abs(c64.calc_energy().e_total - c128.calc_energy().e_total)
+              / abs(c128.calc_energy().e_total)}
+    rt64 = G.B200GrossPitaevskiSolver(p, precision="c64")     # RT only, from the FP64 IT state
+    pert = G.B200GrossPitaevskiSolver(p, precision="c128")    # FP64, start perturbed by 1e-7
+    psi_it = c128.export_data()
+    rt64.load_buffer(psi_it)
+    pert.load_buffer(perturbed(psi_it))
+    runs = {"fp64": c128, "c64_full": c64, "c64_rt_only": rt64, "fp64_perturbed": pert}
+    for s in runs.values():
+        s.init_pote("MEXICAN_FREE")
+    out["readme_fs_128x128x32"] = {"it_1000": it_row,
+                                   "rt": track(runs, "fp64", [1000, 2000, 5000, 10000])}
+    for s in runs.values():
+        s.close()
+
+    # precision study: 256x256x64, FREE, SETUP_GAUSS 3x3x2, edd ramp 1.40 -> 1.60 over 20000
+    j = dict(workload_json("RT"), nx=256, ny=256, nz=64, pote_strategy="FREE",
+             init_strategy="SETUP_GAUSS", bec_droplets_x=3, bec_droplets_y=3, bec_droplets_z=2,
+             iter_real=20000)
+    j.pop("edd")
+    j["edd_start"], j["edd_stop"] = 1.40, 1.60
+    p3 = G.params_from_json(j)
+    runs = {k: G.B200GrossPitaevskiSolver(p3, precision=("c64" if k == "c64" else "c128"))
+            for k in ("fp64", "c64", "fp64_perturbed")}
+    for k, s in runs.items():
+        s.init_pote()
+        s.init_buffer()
+    runs["fp64_perturbed"].load_buffer(perturbed(runs["fp64"].export_data()))
+    out["ramp_256x256x64"] = {"rt": track(runs, "fp64", [1000, 5000, 10000, 20000])}
+    for s in runs.values():
+        s.close()
+    print(json.dumps({"accuracy": out}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -590,7 +686,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="rt", choices=["rt", "sweep"],
+    ap.add_argument("--workload", default="rt", choices=["rt", "sweep", "accuracy"],
                     help="rt: the headline real-time benchmark; sweep: 64 batched imaginary-time solves")
     ap.add_argument("--sweep-members", type=int, default=64)
     ap.add_argument("--sweep-iters", type=int, default=1000)
@@ -605,6 +701,8 @@ def main():
         args.warmup = 3
     if args.workload == "sweep":
         run_sweep(args)
+    elif args.workload == "accuracy":
+        run_accuracy(args)
     elif args.impl == "reference":
         run_reference_arm(args)
     else:

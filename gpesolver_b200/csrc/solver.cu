@@ -1164,9 +1164,11 @@ template <class R> class Solver final : public SolverBase {
         coef_cap = cap;
         if (!coef_event)
             GPE_CUDA(cudaEventCreateWithFlags(&coef_event, cudaEventDisableTiming));
-        // cached RT graphs point at the old coefficient buffer
+        // cached real-time graphs (split schedule: kind 1; fused: kinds 10-12)
+        // hold the address of the old coefficient buffer
         for (auto it = graphs.begin(); it != graphs.end();) {
-            if (std::get<0>(it->first) == 1) {
+            const int kind = std::get<0>(it->first);
+            if (kind == 1 || (kind >= 10 && kind <= 12)) {
                 cudaGraphExecDestroy(it->second);
                 graph_nodes.erase(it->first);
                 it = graphs.erase(it);

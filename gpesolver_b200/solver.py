@@ -275,8 +275,12 @@ class B200GrossPitaevskiSolver:
         if p.calc_strategy in ("IT", "FS"):
             imag_phase()
         if p.calc_strategy == "FS":
+            # SimulationManager::request_free_potential (sim_manager.cpp:78-80):
+            # the caller's potential, else MEXICAN_FREE computed on the device
             if request_free_potential is not None:
                 self.load_pote(request_free_potential())
+            else:
+                self.init_pote("MEXICAN_FREE")
         if p.calc_strategy in ("RT", "FS"):
             real_phase()
 

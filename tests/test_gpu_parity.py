@@ -325,3 +325,24 @@ def test_fused_pipeline_short_runs_match_oracle(dims):
                 s.real_steps(k, 0)
                 assert rel_l2(s.export_data(), want_psi) < 1e-4, sched
                 assert rel_l2(s.export_fi3d(), want_fi) < 1e-4, sched
+
+
+def test_real_steps_after_coefficient_buffer_grows():
+    """A real_steps call longer than any before reallocates the per-iteration
+    coefficient buffer; the cached real-time graphs must not keep reading the
+    old one.  200 + 1500 iterations against 200 + 3 x 500 (different call
+    boundaries change only the rounding of the merged half steps)."""
+    cfg = WELL_CONDITIONED(32, 32, 16)
+    p = gparams(cfg)
+    out = []
+    for calls in ([200, 1500], [200, 500, 500, 500]):
+        with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
+            s.load_pote(G.potential(p))
+            s.load_buffer(G.initial_psi(p))
+            s.imag_steps(20)
+            done = 0
+            for k in calls:
+                s.real_steps(k, done)
+                done += k
+            out.append(s.export_data().copy())
+    assert rel_l2(out[0], out[1]) < 1e-5
