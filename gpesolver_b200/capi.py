@@ -63,6 +63,14 @@ class gpe_init_params(ctypes.Structure):
     ]
 
 
+class gpe_warm_config(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("levels", ctypes.c_int), ("channels", ctypes.c_int * 8),
+        ("hidden", ctypes.c_int), ("n_inputs", ctypes.c_int), ("max_batch", ctypes.c_int),
+    ]
+
+
 # GPE_POT_* (registration order of the reference's potentials) and GPE_INIT_*.
 POTENTIAL_IDS = {"HARMONIC": 0, "MEXICAN": 1, "MEXICAN_FREE": 2, "CYLINDRICAL": 3, "FREE": 4,
                  "MEXICAN_ASYMETRIC": 5, "MEXICAN_ASYMETRIC_FREE": 6}
@@ -111,6 +119,22 @@ SIGNATURES = [
     ("gpe_batch_member", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     ("gpe_batch_set_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("gpe_batch_imag_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
+    ("gpe_warm_create", ctypes.c_int,
+     [ctypes.POINTER(gpe_warm_config), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("gpe_warm_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpe_warm_num_weights", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)]),
+    ("gpe_warm_set_weights", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    ("gpe_warm_get_weights", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    ("gpe_warm_init_weights", ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong]),
+    ("gpe_warm_forward", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    ("gpe_warm_gradients", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+      ctypes.POINTER(ctypes.c_double)]),
+    ("gpe_warm_train_step", ctypes.c_int,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_float,
+      ctypes.POINTER(ctypes.c_double)]),
+    ("gpe_export_amplitude_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    ("gpe_load_amplitude_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     ("gpe_calc_fi3d_noalloc", ctypes.c_int,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
       ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]),

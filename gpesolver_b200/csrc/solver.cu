@@ -136,6 +136,8 @@ class SolverBase {
     virtual void init_potential(const PotCoef &c)            = 0;
     virtual void init_psi(const PsiCoef &c)                  = 0;
     virtual void export_potential(double *out)               = 0;
+    virtual void export_amplitude_device(float *amp)         = 0;
+    virtual void load_amplitude_device(const float *amp)     = 0;
     // batched imaginary time (gpe_batch): the solver's fused IT graph pieces
     // captured as one branch of a batch graph
     virtual bool batchable() const                           = 0;
@@ -155,6 +157,30 @@ static void edd_at(const gpe_params &p, long iter, double *edd, double *ggp11, d
     *edd           = e;
     *ggp11         = 4 * M_PI * a / p.m;
     *gamma         = 128. * std::sqrt(M_PI) * std::pow(a, 2.5) / 3. / p.m * (1. + 1.5 * std::pow(e, 2));
+}
+
+template <class R>
+__global__ void k_amplitude_out(const cplx<R> *__restrict__ psi, const double *__restrict__ divisor,
+                                float *__restrict__ amp, size_t n) {
+    const double sc = 1.0 / sqrt(divisor[0]);
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const cplx<R> p = psi[e];
+        amp[e]          = (float)(sqrt((double)p.x * p.x + (double)p.y * p.y) * sc);
+    }
+}
+
+// psi_0 = max(amp, 0) on the interior, zero on the boundary cells (where the
+// reference's initialisers leave it: imaginary time never updates the boundary,
+// so a non-zero boundary would stay and hold norm)
+__global__ void k_amplitude_in(const float *__restrict__ amp, double *__restrict__ psi_c128, int nx, int ny,
+                               int nz) {
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(e % nz), j = (int)((e / nz) % ny), i = (int)(e / ((size_t)nz * ny));
+        const bool in = i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && k > 0 && k < nz - 1;
+        psi_c128[2 * e]     = in ? fmax((double)amp[e], 0.0) : 0.0;
+        psi_c128[2 * e + 1] = 0.0;
+    }
 }
 
 template <class R> class Solver final : public SolverBase {
@@ -297,6 +323,18 @@ template <class R> class Solver final : public SolverBase {
 
     void init_psi(const PsiCoef &c) override {
         launch(k_init_psi, grid_elem(N), 256, 0, cur, staging.p, geom(), c);
+        load_psi_staged();
+    }
+
+    // |psi| of the normalised psi, FP32, into a device buffer
+    void export_amplitude_device(float *amp) override {
+        launch(k_amplitude_out<R>, grid_elem(N), 256, 0, cur, (const C *)psi.p, (const double *)(norm_state.p + 1),
+               amp, N);
+        GPE_CUDA(cudaStreamSynchronize(cur));
+    }
+    // load_buffer of a real, non-negative amplitude (FP32, device), boundary zero
+    void load_amplitude_device(const float *amp) override {
+        launch(k_amplitude_in, grid_elem(N), 256, 0, cur, amp, staging.p, nx, ny, nz);
         load_psi_staged();
     }
 
@@ -1547,6 +1585,20 @@ int gpe_export_potential(gpe_handle *h, double *V, size_t n) {
     if (!V || n != h->impl->n())
         return bad("potential buffer size mismatch");
     return guarded([&] { h->impl->export_potential(V); });
+}
+
+int gpe_export_amplitude_device(gpe_handle *h, float *amp, size_t n) {
+    GPE_HANDLE(h);
+    if (!amp || n != h->impl->n())
+        return bad("amplitude buffer size mismatch");
+    return guarded([&] { h->impl->export_amplitude_device(amp); });
+}
+
+int gpe_load_amplitude_device(gpe_handle *h, const float *amp, size_t n) {
+    GPE_HANDLE(h);
+    if (!amp || n != h->impl->n())
+        return bad("amplitude buffer size mismatch");
+    return guarded([&] { h->impl->load_amplitude_device(amp); });
 }
 
 int gpe_batch_create(const gpe_params *members, int count, gpe_batch **out) {

@@ -223,6 +223,54 @@ int gpe_batch_set_stream(gpe_batch *b, void *cuda_stream);
 /* k imaginary-time iterations of every member (gpe_imag_steps on each). */
 int gpe_batch_imag_steps(gpe_batch *b, long k);
 
+/* --- learned warm start for imaginary time (no counterpart in the reference) --- */
+
+/* A network maps the physical parameters of a solve (normalised inputs, e.g.
+ * edd, n_atoms, omega_r, omega_z) to an amplitude |psi_0| on the solver grid;
+ * imaginary time refines it instead of starting from an initialiser.
+ *   dense n_inputs -> hidden, SiLU; dense hidden -> channels[0] x latent
+ *   volume (grid / 2^levels), SiLU; `levels` x (nearest x2 upsampling, 3x3x3
+ *   convolution channels[s] -> channels[s+1], SiLU); 3x3x3 convolution
+ *   channels[levels] -> 1 (the amplitude, linear).
+ * Weights BF16, arithmetic FP32; training: mean squared amplitude error, Adam
+ * on FP32 master weights.  Channel counts: 1, 2, 4, 8, 16 or 32. */
+typedef struct gpe_warm_config {
+    int nx, ny, nz;      /* output grid, divisible by 2^levels */
+    int levels;          /* upsampling convolution stages (0..6) */
+    int channels[8];     /* channels[0..levels] */
+    int hidden;          /* width of the first dense layer */
+    int n_inputs;        /* scalar inputs per solve */
+    int max_batch;       /* largest batch of forward / training calls */
+} gpe_warm_config;
+typedef struct gpe_warm gpe_warm;
+int gpe_warm_create(const gpe_warm_config *cfg, int device, gpe_warm **out);
+int gpe_warm_destroy(gpe_warm *w);
+/* number of FP32 weights (the flat layout set / get use) */
+int gpe_warm_num_weights(gpe_warm *w, size_t *n);
+int gpe_warm_set_weights(gpe_warm *w, const float *host, size_t n);
+int gpe_warm_get_weights(gpe_warm *w, float *host, size_t n);
+/* fan-in-scaled uniform initialisation from a seed (host generator) */
+int gpe_warm_init_weights(gpe_warm *w, unsigned long long seed);
+/* amplitudes of B solves (inputs B x n_inputs on the host) into amp_dev
+ * (device, B x nx*ny*nz floats) */
+int gpe_warm_forward(gpe_warm *w, const float *inputs, int B, float *amp_dev);
+/* loss and gradient (host, num_weights floats; NULL: kept on the device) of
+ * the mean squared error against targets_dev (device, B x nx*ny*nz) */
+int gpe_warm_gradients(gpe_warm *w, const float *inputs, const float *targets_dev, int B, float *grad,
+                       double *loss);
+/* one Adam step on a batch */
+int gpe_warm_train_step(gpe_warm *w, const float *inputs, const float *targets_dev, int B, float lr,
+                        double *loss);
+
+/* Amplitude |psi| of the handle's (normalised) psi into a device buffer (FP32),
+ * and load_buffer of a real amplitude given on the device (FP32): the hand-off
+ * between a solver and the warm-start network without a host round trip.  The
+ * loaded state is max(amp, 0) on the interior and zero on the boundary cells,
+ * as the reference's initialisers leave them (initializer.cpp:46-219);
+ * imaginary time never updates the boundary. */
+int gpe_export_amplitude_device(gpe_handle *h, float *amp_dev, size_t n);
+int gpe_load_amplitude_device(gpe_handle *h, const float *amp_dev, size_t n);
+
 /* --- allocation-free variant --- */
 
 /* Size of the file-scope device array gpe_calc_fi3d_noalloc works in. */
