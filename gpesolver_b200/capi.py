@@ -96,6 +96,8 @@ SIGNATURES = [
     ("gpe_load_potential", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     ("gpe_export_psi", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     ("gpe_export_fi3d", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
+    ("gpe_export_psi_async", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
+    ("gpe_export_wait", ctypes.c_int, [ctypes.c_void_p]),
     ("gpe_calc_fi3d", ctypes.c_int, [ctypes.c_void_p]),
     ("gpe_imag_iter_linear_step", ctypes.c_int, [ctypes.c_void_p]),
     ("gpe_imag_iter_nonlinear_step", ctypes.c_int, [ctypes.c_void_p]),

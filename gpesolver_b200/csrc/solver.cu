@@ -137,6 +137,8 @@ class SolverBase {
     virtual void init_psi(const PsiCoef &c)                  = 0;
     virtual void export_potential(double *out)               = 0;
     virtual void export_amplitude_device(float *amp)         = 0;
+    virtual void export_psi_async(double *host)              = 0;
+    virtual void export_wait()                               = 0;
     virtual void load_amplitude_device(const float *amp)     = 0;
     // batched imaginary time (gpe_batch): the solver's fused IT graph pieces
     // captured as one branch of a batch graph
@@ -259,6 +261,12 @@ template <class R> class Solver final : public SolverBase {
     }
 
     ~Solver() override {
+        if (ev_copied) {
+            cudaEventSynchronize(ev_copied);
+            cudaEventDestroy(ev_copied);
+            cudaEventDestroy(ev_widened);
+            cudaStreamDestroy(copy_stream);
+        }
         for (auto &kv : graphs)
             cudaGraphExecDestroy(kv.second);
         if (coef_host)
@@ -324,6 +332,31 @@ template <class R> class Solver final : public SolverBase {
     void init_psi(const PsiCoef &c) override {
         launch(k_init_psi, grid_elem(N), 256, 0, cur, staging.p, geom(), c);
         load_psi_staged();
+    }
+
+    // export_psi without waiting: psi is widened to complex128 on the device into
+    // a buffer of its own (on the compute stream, before any later iteration),
+    // then copied to `host` on a copy stream while the compute stream goes on.
+    // `host` should be pinned for the copy to overlap.
+    void export_psi_async(double *host) override {
+        if (!export_buf.p) {
+            export_buf.alloc(2 * N);
+            GPE_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+            GPE_CUDA(cudaEventCreateWithFlags(&ev_widened, cudaEventDisableTiming));
+            GPE_CUDA(cudaEventCreateWithFlags(&ev_copied, cudaEventDisableTiming));
+        } else {
+            GPE_CUDA(cudaEventSynchronize(ev_copied)); // the buffer of the previous export
+        }
+        launch(k_to_f64<R>, grid_elem(2 * N), 256, 0, cur, reinterpret_cast<const R *>(psi.p), export_buf.p,
+               2 * N, (const double *)(norm_state.p + 1), 1);
+        GPE_CUDA(cudaEventRecord(ev_widened, cur));
+        GPE_CUDA(cudaStreamWaitEvent(copy_stream, ev_widened, 0));
+        GPE_CUDA(cudaMemcpyAsync(host, export_buf.p, sizeof(double) * 2 * N, cudaMemcpyDeviceToHost, copy_stream));
+        GPE_CUDA(cudaEventRecord(ev_copied, copy_stream));
+    }
+    void export_wait() override {
+        if (export_buf.p)
+            GPE_CUDA(cudaEventSynchronize(ev_copied));
     }
 
     // |psi| of the normalised psi, FP32, into a device buffer
@@ -1029,6 +1062,9 @@ template <class R> class Solver final : public SolverBase {
     DevBuf<C> psi, psii, bnd, A, ex, ey, ez;
     DevBuf<R> V, phi, vk;
     DevBuf<double> staging, norm_state, partial, epartial, eout;
+    DevBuf<double> export_buf; // asynchronous exports
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_widened = nullptr, ev_copied = nullptr;
     DevBuf<int> status, iter_zero, iter_base;
     // fused pipeline (compile-time line lengths; complex64 only)
     bool fused = false;
@@ -1585,6 +1621,18 @@ int gpe_export_potential(gpe_handle *h, double *V, size_t n) {
     if (!V || n != h->impl->n())
         return bad("potential buffer size mismatch");
     return guarded([&] { h->impl->export_potential(V); });
+}
+
+int gpe_export_psi_async(gpe_handle *h, double *psi_c128, size_t n) {
+    GPE_HANDLE(h);
+    if (!psi_c128 || n != h->impl->n())
+        return bad("psi buffer size mismatch");
+    return guarded([&] { h->impl->export_psi_async(psi_c128); });
+}
+
+int gpe_export_wait(gpe_handle *h) {
+    GPE_HANDLE(h);
+    return guarded([&] { h->impl->export_wait(); });
 }
 
 int gpe_export_amplitude_device(gpe_handle *h, float *amp, size_t n) {

@@ -170,6 +170,16 @@ class B200GrossPitaevskiSolver:
         capi.check(self._L.gpe_export_psi(self._h, capi.dptr(out), self.n))
         return out.view(np.complex128).reshape(self.params.shape)
 
+    def export_async(self, buf: np.ndarray) -> None:
+        """Start copying psi (complex128, flat float64 view of 2n values) into
+        `buf` (pinned host memory) without waiting; export_wait() completes it."""
+        if buf.dtype != np.float64 or buf.size != 2 * self.n or not buf.flags["C_CONTIGUOUS"]:
+            raise capi.GpeError(capi.GPE_ERR_ARG, "export buffer must be 2n contiguous float64")
+        capi.check(self._L.gpe_export_psi_async(self._h, capi.dptr(buf), self.n))
+
+    def export_wait(self) -> None:
+        capi.check(self._L.gpe_export_wait(self._h))
+
     def export_fi3d(self) -> np.ndarray:
         out = np.zeros(self.n)
         capi.check(self._L.gpe_export_fi3d(self._h, capi.dptr(out), self.n))
@@ -240,49 +250,72 @@ class B200GrossPitaevskiSolver:
 
     # -- driver (AbstractGrossPitaevskiSolver::solve, solver.cpp:25-97) -----
     def solve(self, checkpoint: Optional[Callable[[str, int, np.ndarray], None]] = None,
-              request_free_potential: Optional[Callable[[], np.ndarray]] = None) -> None:
-        """Runs the configured strategy with the reference's cadence: energies
-        and checkpoints after iterations 0, 100, 200, ... (IT) and 0, 1000, ...
-        (RT); the FS strategy switches to the free potential in between."""
+              request_free_potential: Optional[Callable[[], np.ndarray]] = None,
+              checkpointer=None, resume: Optional[dict] = None) -> None:
+        """Runs the configured strategy with the reference's cadence
+        (solver.cpp:25-97): energies and checkpoints after iterations 0, 100,
+        200, ... (IT) and 0, 1000, ... (RT); the FS strategy switches to the free
+        potential in between.
+
+        checkpoint(phase, iteration, psi): called with psi on the host at every
+        checkpoint (synchronous, as the reference's save_checkpoint).
+        checkpointer: a checkpoint.Checkpointer instead -- the copy of psi
+        overlaps the next iterations and the file is written in the background.
+        resume: {"phase": "imag" | "real", "iteration": it} of a checkpoint whose
+        psi has been loaded (load_buffer): the run continues after it, the edd
+        ramp included."""
         p = self.params
 
-        def imag_phase():
-            done = 0
+        def at_checkpoint(phase, it):
+            if checkpointer is not None:
+                checkpointer.checkpoint(phase, it)
+            elif checkpoint:
+                checkpoint(phase, it, self.export_data())
+            self.calc_energy()
+
+        def imag_phase(done):
             total = p.iter_imag + 1
             while done < total:
-                k = 1 if done == 0 else min(100, total - done)
+                k = 1 if done == 0 else min(100 - (done - 1) % 100, total - done)
                 self.imag_steps(k)
                 done += k
                 it = done - 1
                 if it % 100 == 0:
-                    if checkpoint:
-                        checkpoint("imag", it, self.export_data())
-                    self.calc_energy()
+                    at_checkpoint("imag", it)
 
-        def real_phase():
-            done = 0
+        def real_phase(done):
             total = p.iter_real + 1
             while done < total:
-                k = 1 if done == 0 else min(1000, total - done)
+                k = 1 if done == 0 else min(1000 - (done - 1) % 1000, total - done)
                 self.real_steps(k, done)
                 done += k
                 it = done - 1
                 if it % 1000 == 0:
-                    if checkpoint:
-                        checkpoint("real", it, self.export_data())
-                    self.calc_energy()
+                    at_checkpoint("real", it)
 
-        if p.calc_strategy in ("IT", "FS"):
-            imag_phase()
-        if p.calc_strategy == "FS":
+        phase0, start = "imag", 0
+        if resume is not None:
+            phase0, start = resume["phase"], int(resume["iteration"]) + 1
+        if p.calc_strategy in ("IT", "FS") and phase0 == "imag":
+            imag_phase(start)
+            start = 0
+        if p.calc_strategy == "FS" and phase0 == "imag":
             # SimulationManager::request_free_potential (sim_manager.cpp:78-80):
             # the caller's potential, else MEXICAN_FREE computed on the device
             if request_free_potential is not None:
                 self.load_pote(request_free_potential())
             else:
                 self.init_pote("MEXICAN_FREE")
+        if p.calc_strategy == "FS" and phase0 == "real":
+            # resumed after the switch: the free potential again
+            if request_free_potential is not None:
+                self.load_pote(request_free_potential())
+            else:
+                self.init_pote("MEXICAN_FREE")
         if p.calc_strategy in ("RT", "FS"):
-            real_phase()
+            real_phase(start)
+        if checkpointer is not None:
+            checkpointer.close()
 
 
 def _as_c128_flat(psi, n: int) -> np.ndarray:

@@ -117,6 +117,15 @@ int gpe_load_potential(gpe_handle *h, const double *V, size_t n);
 /* export_data: the current psi (normalised if the last step was an imaginary-time
  * step), widened to complex128. */
 int gpe_export_psi(gpe_handle *h, double *psi_c128, size_t n);
+/* gpe_export_psi without waiting for the copy: psi is widened to complex128 on
+ * the device (before any later call's iterations), then copied to psi_c128 on
+ * a copy stream of the handle, overlapping the iterations that follow.  Use
+ * pinned host memory for the overlap; the buffer must stay valid until
+ * gpe_export_wait returns.  A second call waits for the first copy.  (The
+ * reference copies psi synchronously at every checkpoint, solver.cpp:54-59,
+ * 81-86.) */
+int gpe_export_psi_async(gpe_handle *h, double *psi_c128, size_t n);
+int gpe_export_wait(gpe_handle *h);
 /* The dipolar field fi3d as last computed (FP64 copy). */
 int gpe_export_fi3d(gpe_handle *h, double *fi3d, size_t n);
 

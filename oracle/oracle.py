@@ -311,6 +311,9 @@ def rlib():
         L.gperef_change_potential.argtypes = [ctypes.c_char_p]
         L.gperef_op.argtypes = [ctypes.c_int]
         L.gperef_solve.argtypes = [ctypes.c_int]
+        for name in ("gperef_save_binary", "gperef_save_text", "gperef_save_pote_text"):
+            getattr(L, name).argtypes = [ctypes.c_char_p]
+        L.gperef_load_binary.argtypes = [ctypes.c_char_p, _dp]
         L.gperef_checkpoints.restype = ctypes.c_long
         L.gperef_saved_energies.restype = ctypes.c_long
         L.gperef_saved_energies.argtypes = [_dp, ctypes.c_long]
@@ -427,6 +430,27 @@ class RefSolver:
 
     def saved_energies(self) -> np.ndarray:
         return _saved_energies(rlib().gperef_saved_energies)
+
+
+    # the reference's FileManager (names without extension; energies into the
+    # working directory's energy.gpe.dat)
+    def save_binary(self, name: str):
+        assert rlib().gperef_save_binary(name.encode()) == 0, rlib().gperef_last_error()
+
+    def save_text(self, name: str):
+        assert rlib().gperef_save_text(name.encode()) == 0, rlib().gperef_last_error()
+
+    def save_pote_text(self, name: str):
+        assert rlib().gperef_save_pote_text(name.encode()) == 0, rlib().gperef_last_error()
+
+    def save_energies(self):
+        assert rlib().gperef_save_energies() == 0, rlib().gperef_last_error()
+
+    def load_binary(self, name: str) -> np.ndarray:
+        out = np.zeros(2 * self.n)
+        if rlib().gperef_load_binary(name.encode(), _ptr(out)) != 0:
+            raise RuntimeError(rlib().gperef_last_error().decode())
+        return out
 
 
 def _saved_energies(fn) -> np.ndarray:

@@ -15,6 +15,7 @@
 // src/parameters/potentials.hpp:76-157), linked against the FP64 FFTW-API shim in
 // oracle/fftw_shim.
 #include "context/context.hpp"
+#include "filemanager/file_manager.hpp"
 #include "initializer/initializer.hpp"
 #include "manager/sim_mediator.hpp"
 #include "parameters/parameters.hpp"
@@ -283,6 +284,70 @@ int gperef_export_pote(double *out) {
     const potential_t &v = g_state->solver->buf().pote;
     std::memcpy(out, v.get_data(), sizeof(double) * v.size());
     return 0;
+}
+
+// The reference's FileManager writers and reader (src/filemanager/file_manager.cpp:81-112,
+// 251-290, 387-401, 404-434), on the harness's current psi / potential / energies.
+// `name` has no extension (the writer appends it); energies go to
+// energy.gpe.dat in the working directory.
+int gperef_save_binary(const char *name) {
+    if (!g_state) return 1;
+    try {
+        FileManager fm(&g_state->mediator);
+        g_state->solver->export_data();
+        fm.save_to_binary_file(g_state->solver->buf().cpsi, name);
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+int gperef_save_text(const char *name) {
+    if (!g_state) return 1;
+    try {
+        FileManager fm(&g_state->mediator);
+        g_state->solver->export_data();
+        fm.save_to_text_file(g_state->solver->buf().cpsi, name);
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+int gperef_save_pote_text(const char *name) {
+    if (!g_state) return 1;
+    try {
+        FileManager fm(&g_state->mediator);
+        fm.save_pote_to_text_file(g_state->solver->buf().pote, name);
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+int gperef_save_energies(void) {
+    if (!g_state) return 1;
+    try {
+        FileManager fm(&g_state->mediator);
+        fm.save_energies(g_state->mediator.energies);
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// FileManager::load_from_binary_file (file_manager.cpp:292-335) into out (2n doubles).
+int gperef_load_binary(const char *name, double *out) {
+    if (!g_state) return 1;
+    try {
+        FileManager fm(&g_state->mediator);
+        fm.load_from_binary_file(name, [&](wavefunction_t &w) {
+            std::memcpy(out, w.get_data(), sizeof(double) * 2 * w.size());
+        });
+        return 0;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
 }
 
 // {e_kin, e_pot, e_int, e_ext (dipolar), e_bmf, e_total} after calc_energy.
