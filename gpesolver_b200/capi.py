@@ -108,6 +108,7 @@ SIGNATURES = [
     ("gpe_calc_energy", ctypes.c_int, [ctypes.c_void_p, _dp]),
     ("gpe_set_coeffs", ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]),
     ("gpe_imag_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_long]),
+    ("gpe_imag_steps_energies", ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, _dp]),
     ("gpe_real_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, ctypes.c_long]),
     ("gpe_launch_count", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
     ("gpe_time_kernel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]),

@@ -127,6 +127,7 @@ class SolverBase {
     virtual void energy(double *out6)                        = 0;
     virtual void set_coeffs(double ggp11, double gamma)      = 0;
     virtual void imag_steps(long k)                          = 0;
+    virtual void imag_steps_energies(long k, int checks, double *e_total) = 0;
     virtual void real_steps(long k, long first_iter)         = 0;
     virtual long long launches() const                       = 0;
     virtual void time_kernel(int which, int reps, double *ms, double *bytes) = 0;
@@ -487,6 +488,47 @@ template <class R> class Solver final : public SolverBase {
         for (int t = 0; t < 6; ++t)
             if (!std::isfinite(out[t]))
                 throw Error(GPE_ERR_NUMERIC, "non-finite energy");
+    }
+
+    // `checks` times: k imaginary-time iterations, then the total energy into a
+    // device history; one host synchronisation at the end.
+    void imag_steps_energies(long k, int checks, double *e_total) override {
+        if (k <= 0 || checks <= 0)
+            throw Error(GPE_ERR_ARG, "iterations and checks must be positive");
+        if (ehist.n < (size_t)5 * checks)
+            ehist.alloc((size_t)5 * checks);
+        const int nb = nblk_elem;
+        for (int c = 0; c < checks; ++c) {
+            if (!lazy)
+                set_divisor_one();
+            if (fused) {
+                fused_imag(k);
+            } else {
+                long done = 0;
+                while (k - done >= kItChunk) {
+                    run_graph(0, kItChunk);
+                    done += kItChunk;
+                }
+                if (k - done > 0)
+                    run_graph(0, (int)(k - done));
+            }
+            lazy = true;
+            launch(k_energy_partial<R>, nb, 256, 0, cur, (const C *)psi.p, (const R *)V.p, (const R *)phi.p,
+                   (const double *)(norm_state.p + 1), 1, epartial.p, nx, ny, nz, 1.0 / (P.dx * P.dx),
+                   1.0 / (P.dy * P.dy), 1.0 / (P.dz * P.dz), ggp11_cur, P.cdd, P.n_atoms, gamma_cur);
+            launch(k_energy_finalize, 1, 256, 0, cur, (const double *)epartial.p, nb, ehist.p + 5 * c);
+        }
+        std::vector<double> e((size_t)5 * checks);
+        GPE_CUDA(cudaMemcpyAsync(e.data(), ehist.p, sizeof(double) * e.size(), cudaMemcpyDeviceToHost, cur));
+        check_status();
+        const double dV = P.dx * P.dy * P.dz, w = P.n_atoms;
+        for (int c = 0; c < checks; ++c) {
+            const double *x = &e[(size_t)5 * c];
+            e_total[c] = x[0] * (dV / (2 * P.m) * w) + x[1] * (dV * w) + x[2] * (dV * std::pow(w, 2)) + x[3] * dV +
+                         x[4] * (dV * std::pow(w, 2.5));
+            if (!std::isfinite(e_total[c]))
+                throw Error(GPE_ERR_NUMERIC, "non-finite energy");
+        }
     }
 
     void set_coeffs(double ggp11, double gamma) override {
@@ -1063,6 +1105,7 @@ template <class R> class Solver final : public SolverBase {
     DevBuf<R> V, phi, vk;
     DevBuf<double> staging, norm_state, partial, epartial, eout;
     DevBuf<double> export_buf; // asynchronous exports
+    DevBuf<double> ehist;      // energy history of imag_steps_energies
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_widened = nullptr, ev_copied = nullptr;
     DevBuf<int> status, iter_zero, iter_base;
@@ -1621,6 +1664,13 @@ int gpe_export_potential(gpe_handle *h, double *V, size_t n) {
     if (!V || n != h->impl->n())
         return bad("potential buffer size mismatch");
     return guarded([&] { h->impl->export_potential(V); });
+}
+
+int gpe_imag_steps_energies(gpe_handle *h, long k, int checks, double *e_total) {
+    GPE_HANDLE(h);
+    if (!e_total)
+        return bad("null argument");
+    return guarded([&] { h->impl->imag_steps_energies(k, checks, e_total); });
 }
 
 int gpe_export_psi_async(gpe_handle *h, double *psi_c128, size_t n) {

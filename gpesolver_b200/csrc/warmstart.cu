@@ -147,40 +147,111 @@ __device__ __forceinline__ float conv_in(const float *__restrict__ in, const Con
 
 constexpr int kMaxCout = 32;
 
-// one thread per output voxel, all output channels; weights [o][c][27] BF16
-// staged in shared memory as FP32.  pre = the pre-activation, out = SiLU(pre)
-// (act = 0: out = pre).  blockIdx.y = batch sample.
+// one thread per output voxel and group of COUT output channels (blockIdx.y =
+// sample * groups + group: small volumes spread their channels over more
+// threads); weights [o][c][27] BF16 staged in shared memory as FP32.  pre =
+// the pre-activation, out = SiLU(pre) (act = 0: out = pre).
 template <int COUT>
 __global__ void k_conv_fwd(const float *__restrict__ in, const __nv_bfloat16 *__restrict__ W,
                            const __nv_bfloat16 *__restrict__ bias, float *__restrict__ pre,
                            float *__restrict__ out, ConvGeom g, int act, size_t in_stride, size_t out_stride) {
+    const int groups = g.cout / COUT;
+    const int smp = blockIdx.y / groups, o0 = (blockIdx.y % groups) * COUT;
     extern __shared__ float ws[];
     const int nw = g.cout * g.cin * 27;
     for (int e = threadIdx.x; e < nw; e += blockDim.x)
         ws[e] = __bfloat162float(W[e]);
     __syncthreads();
     const size_t nv = (size_t)g.X * g.Y * g.Z;
-    const float *inb = in + blockIdx.y * in_stride;
+    const float *inb = in + smp * in_stride;
     for (size_t v = blockIdx.x * (size_t)blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
         const int z = (int)(v % g.Z), y = (int)((v / g.Z) % g.Y), x = (int)(v / ((size_t)g.Z * g.Y));
         float acc[COUT];
 #pragma unroll
         for (int o = 0; o < COUT; ++o)
-            acc[o] = __bfloat162float(bias[o]);
+            acc[o] = __bfloat162float(bias[o0 + o]);
         for (int c = 0; c < g.cin; ++c)
             for (int t = 0; t < 27; ++t) {
                 const int dx = t / 9 - 1, dy = (t / 3) % 3 - 1, dz = t % 3 - 1;
                 const float u = conv_in(inb, g, c, x + dx, y + dy, z + dz);
 #pragma unroll
                 for (int o = 0; o < COUT; ++o)
-                    acc[o] = fmaf(ws[(o * g.cin + c) * 27 + t], u, acc[o]);
+                    acc[o] = fmaf(ws[((o0 + o) * g.cin + c) * 27 + t], u, acc[o]);
             }
 #pragma unroll
         for (int o = 0; o < COUT; ++o) {
-            const size_t q = blockIdx.y * out_stride + (size_t)o * nv + v;
+            const size_t q = smp * out_stride + (size_t)(o0 + o) * nv + v;
             pre[q]         = acc[o];
             out[q]         = act ? silu(acc[o]) : acc[o];
         }
+    }
+}
+
+// The same convolution on 8x8x8 output tiles, one voxel per thread (512
+// threads): the input tile with its halo is staged in shared memory once
+// (zeros outside the volume), the 27 taps and CIN channels unroll, so a voxel
+// costs CIN x 27 shared loads and CIN x 27 x COUT FMAs without per-tap index
+// arithmetic.  For volumes with all sizes multiples of 8 and the channel
+// counts instantiated below.  blockIdx.y = sample.
+template <int CIN, int COUT, int UP>
+__global__ void __launch_bounds__(512)
+    k_conv_fwd_tile(const float *__restrict__ in, const __nv_bfloat16 *__restrict__ W,
+                    const __nv_bfloat16 *__restrict__ bias, float *__restrict__ pre, float *__restrict__ out,
+                    ConvGeom g, int act, size_t in_stride, size_t out_stride) {
+    constexpr int T = UP ? 6 : 10; // staged input tile edge
+    __shared__ float ws[COUT * CIN * 27];
+    __shared__ float ts[CIN * T * T * T];
+    const int tid = threadIdx.x;
+    for (int e = tid; e < COUT * CIN * 27; e += 512)
+        ws[e] = __bfloat162float(W[e]);
+    const int tx = g.X / 8, ty = g.Y / 8;
+    const int bx = blockIdx.x / (ty * (g.Z / 8)), rem = blockIdx.x % (ty * (g.Z / 8));
+    const int by = rem / (g.Z / 8), bz = rem % (g.Z / 8);
+    (void)tx;
+    const int x0 = bx * 8, y0 = by * 8, z0 = bz * 8;
+    const float *inb = in + blockIdx.y * in_stride;
+    // input origin of the tile (coarse grid when UP)
+    const int Xi = UP ? g.X / 2 : g.X, Yi = UP ? g.Y / 2 : g.Y, Zi = UP ? g.Z / 2 : g.Z;
+    const int ox = UP ? x0 / 2 - 1 : x0 - 1, oy = UP ? y0 / 2 - 1 : y0 - 1, oz = UP ? z0 / 2 - 1 : z0 - 1;
+    for (int e = tid; e < CIN * T * T * T; e += 512) {
+        const int c = e / (T * T * T), r = e % (T * T * T);
+        const int ix = ox + r / (T * T), iy = oy + (r / T) % T, iz = oz + r % T;
+        float v = 0.f;
+        if (ix >= 0 && iy >= 0 && iz >= 0 && ix < Xi && iy < Yi && iz < Zi)
+            v = __ldg(&inb[(((size_t)c * Xi + ix) * Yi + iy) * Zi + iz]);
+        ts[e] = v;
+    }
+    __syncthreads();
+    const int lx = tid / 64, ly = (tid / 8) % 8, lz = tid % 8;
+    // tile offsets of the three neighbours along each axis
+    int ax[3], ay[3], az[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        ax[d] = UP ? ((lx + d - 1) >> 1) + 1 : lx + d;
+        ay[d] = UP ? ((ly + d - 1) >> 1) + 1 : ly + d;
+        az[d] = UP ? ((lz + d - 1) >> 1) + 1 : lz + d;
+    }
+    float acc[COUT];
+#pragma unroll
+    for (int o = 0; o < COUT; ++o)
+        acc[o] = __bfloat162float(bias[o]);
+#pragma unroll
+    for (int c = 0; c < CIN; ++c) {
+#pragma unroll
+        for (int t = 0; t < 27; ++t) {
+            const float u = ts[c * T * T * T + (ax[t / 9] * T + ay[(t / 3) % 3]) * T + az[t % 3]];
+#pragma unroll
+            for (int o = 0; o < COUT; ++o)
+                acc[o] = fmaf(ws[(o * CIN + c) * 27 + t], u, acc[o]);
+        }
+    }
+    const size_t nv = (size_t)g.X * g.Y * g.Z;
+    const size_t v  = ((size_t)(x0 + lx) * g.Y + (y0 + ly)) * g.Z + (z0 + lz);
+#pragma unroll
+    for (int o = 0; o < COUT; ++o) {
+        const size_t q = blockIdx.y * out_stride + (size_t)o * nv + v;
+        pre[q]         = acc[o];
+        out[q]         = act ? silu(acc[o]) : acc[o];
     }
 }
 
@@ -410,8 +481,45 @@ void forward(gpe_warm *W, int B) {
         const size_t n = W->vox((int)l) * L.cout;
         const size_t sm = sizeof(float) * L.cin * L.cout * 27;
         const int last  = l + 1 == W->conv.size();
-        gpe::by_channels(L.cout, [&](auto CO) {
-            k_conv_fwd<decltype(CO)::value><<<dim3(gpe::grid_for(W->vox((int)l)), B), 256, sm, s>>>(
+        const size_t nvox = W->vox((int)l);
+        if (L.g.X % 8 == 0 && L.g.Y % 8 == 0 && L.g.Z % 8 == 0 && nvox >= 32768) {
+            const int tiles = (L.g.X / 8) * (L.g.Y / 8) * (L.g.Z / 8);
+            bool done = false;
+            auto go = [&](auto CI, auto CO, auto UPc) {
+                constexpr int ci = decltype(CI)::value, co = decltype(CO)::value, up = decltype(UPc)::value;
+                if (L.cin == ci && L.cout == co && L.g.up == up) {
+                    gpe::k_conv_fwd_tile<ci, co, up><<<dim3(tiles, B), 512, 0, s>>>(
+                        in, wb + L.w, wb + L.b, W->pre[l].p, W->act[l].p, L.g, last ? 0 : 1, in_stride, n);
+                    done = true;
+                }
+            };
+            using I4 = std::integral_constant<int, 4>;
+            using I8 = std::integral_constant<int, 8>;
+            using I16 = std::integral_constant<int, 16>;
+            using I1 = std::integral_constant<int, 1>;
+            using U0 = std::integral_constant<int, 0>;
+            using U1 = std::integral_constant<int, 1>;
+            go(I16{}, I8{}, U1{});
+            go(I8{}, I8{}, U1{});
+            go(I8{}, I4{}, U1{});
+            go(I4{}, I4{}, U1{});
+            go(I8{}, I1{}, U0{});
+            go(I4{}, I1{}, U0{});
+            go(I8{}, I8{}, U0{});
+            if (done) {
+                in        = W->act[l].p;
+                in_stride = n;
+                continue;
+            }
+        }
+        // output channels per thread: all of them on large volumes, fewer on
+        // small ones, so that a layer runs at least ~64 k threads
+        int per = L.cout;
+        while (per > 1 && nvox * B * (L.cout / per) < 65536)
+            per >>= 1;
+        const int groups = L.cout / per;
+        gpe::by_channels(per, [&](auto CO) {
+            k_conv_fwd<decltype(CO)::value><<<dim3(gpe::grid_for(nvox), B * groups), 256, sm, s>>>(
                 in, wb + L.w, wb + L.b, W->pre[l].p, W->act[l].p, L.g, last ? 0 : 1, in_stride, n);
         });
         in        = W->act[l].p;

@@ -243,6 +243,13 @@ class B200GrossPitaevskiSolver:
     def imag_steps(self, k: int) -> None:
         capi.check(self._L.gpe_imag_steps(self._h, int(k)))
 
+    def imag_steps_energies(self, k: int, checks: int) -> np.ndarray:
+        """`checks` rounds of k imaginary-time iterations; the total energy after
+        each round (one host synchronisation for all of them)."""
+        out = np.zeros(checks)
+        capi.check(self._L.gpe_imag_steps_energies(self._h, int(k), int(checks), capi.dptr(out)))
+        return out
+
     def real_steps(self, k: int, first_iter: int = 0) -> None:
         capi.check(self._L.gpe_real_steps(self._h, int(k), int(first_iter)))
         if not self.params.const_edd and k > 0:

@@ -154,6 +154,13 @@ int gpe_imag_steps(gpe_handle *h, long k);
  * handle's const_edd is 0 (calc_evolution, solver.cpp:75-77). */
 int gpe_real_steps(gpe_handle *h, long k, long first_iter);
 
+/* `checks` rounds of (k imaginary-time iterations, calc_energy), with the
+ * energies kept on the device until the end: e_total[c] = the total energy
+ * after round c.  One host synchronisation instead of one per check (the
+ * reference's calc_initial_state computes the energy every 100 iterations,
+ * solver.cpp:54-59; a convergence loop checks it more often). */
+int gpe_imag_steps_energies(gpe_handle *h, long k, int checks, double *e_total);
+
 /* Number of kernels the library launched on this handle since creation. */
 int gpe_launch_count(gpe_handle *h, long long *count);
 

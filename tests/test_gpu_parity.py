@@ -346,3 +346,21 @@ def test_real_steps_after_coefficient_buffer_grows():
                 done += k
             out.append(s.export_data().copy())
     assert rel_l2(out[0], out[1]) < 1e-5
+
+
+def test_energy_history_equals_per_check_energies():
+    """imag_steps_energies keeps the energies on the device between host
+    synchronisations: the same numbers as stepping and calling calc_energy."""
+    cfg = WELL_CONDITIONED(32, 32, 16)
+    p = gparams(cfg)
+    with G.B200GrossPitaevskiSolver(p) as a, G.B200GrossPitaevskiSolver(p) as b:
+        for s in (a, b):
+            s.load_pote(G.potential(p))
+            s.load_buffer(G.initial_psi(p))
+        hist = a.imag_steps_energies(10, 6)
+        want = []
+        for _ in range(6):
+            b.imag_steps(10)
+            want.append(b.calc_energy().e_total)
+        np.testing.assert_array_equal(hist, want)
+        np.testing.assert_array_equal(a.export_data(), b.export_data())

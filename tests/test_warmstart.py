@@ -18,17 +18,20 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-@pytest.mark.parametrize("levels,channels", [(2, (4, 4, 2)), (1, (8, 2))])
-def test_gradients_match_fp64_restatement(levels, channels):
+@pytest.mark.parametrize("dims,levels,channels", [((16, 16, 8), 2, (4, 4, 2)), ((16, 16, 8), 1, (8, 2)),
+                                                   ((32, 32, 32), 2, (4, 8, 8))])
+def test_gradients_match_fp64_restatement(dims, levels, channels):
+    """(32^3: the large layers take the tiled forward convolution.)"""
     import torch
 
-    cfg = W.WarmConfig(nx=16, ny=16, nz=8, levels=levels, channels=channels, hidden=8, max_batch=3)
+    nx, ny, nz = dims
+    cfg = W.WarmConfig(nx=nx, ny=ny, nz=nz, levels=levels, channels=channels, hidden=8, max_batch=3)
     net = W.WarmStartNet(cfg, seed=5)
-    ref = WarmNetRef(16, 16, 8, levels, channels, hidden=8)
+    ref = WarmNetRef(nx, ny, nz, levels, channels, hidden=8)
     assert net.n_weights == ref.n_weights
     rng = np.random.default_rng(2)
     x = rng.uniform(-1, 1, (3, 4)).astype(np.float32)
-    t = rng.uniform(0, 2, (3, 16 * 16 * 8)).astype(np.float32)
+    t = rng.uniform(0, 2, (3, nx * ny * nz)).astype(np.float32)
     td = torch.tensor(t, device="cuda")
     loss, g = net.gradients(x, td.data_ptr())
     rloss, rg = ref.loss_and_grad(net.get_weights(), x, t)
@@ -36,7 +39,7 @@ def test_gradients_match_fp64_restatement(levels, channels):
     for name, (o, n) in ref.off.items():
         assert _rel(g[o:o + n], rg[o:o + n]) < 2e-4, name
     # forward: the amplitudes themselves
-    amp = torch.empty(3 * 16 * 16 * 8, device="cuda")
+    amp = torch.empty(3 * nx * ny * nz, device="cuda")
     net.forward(x, amp.data_ptr())
     net.close()
 
