@@ -69,52 +69,33 @@ def config_dict() -> dict:
 # distributed plumbing
 # ---------------------------------------------------------------------------
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from gpesolver_b200 import replicas
+
+    return replicas.env()
 
 
 def dist_init(ws, local):
-    import torch
+    from gpesolver_b200 import replicas
 
-    if ws > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    replicas.init(ws, local, "nccl")
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
+    from gpesolver_b200 import replicas
 
-        dist.barrier()
+    replicas.barrier(ws)
 
 
 def max_over_ranks(ws, x: float) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from gpesolver_b200 import replicas
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.reduce(ws, x, "max")
 
 
 def sum_over_ranks(ws, x: float) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from gpesolver_b200 import replicas
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return replicas.reduce(ws, x, "sum")
 
 
 # ---------------------------------------------------------------------------
@@ -180,12 +161,13 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baselines (the reference's own CPU code)
 # ---------------------------------------------------------------------------
-def reference_cpu_rate(budget_s: float, min_iters: int = 3, max_iters: int = 200) -> dict:
+def reference_cpu_rate(budget_s: float, min_iters: int = 3, max_iters: int = 200, threads: int = 0) -> dict:
     """RT iterations/s of the reference's CpuGrossPitaevskiSolver on the workload,
-    from the state after 2 IT iterations (a bounded sample of the full run)."""
+    from the state after 2 IT iterations (a bounded sample of the full run);
+    threads = fftw_n_threads (0: every host core)."""
     from oracle import oracle as O
 
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     cfg = O.default_config(nx=NX, ny=NY, nz=NZ, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
                            pote_strategy="MEXICAN", fftw_n_threads=threads)
     kind = "reference" if O.ref_available() else "port"
@@ -202,6 +184,30 @@ def reference_cpu_rate(budget_s: float, min_iters: int = 3, max_iters: int = 200
     return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": kind,
             "sample": f"{n} RT iterations at {NX}x{NY}x{NZ} after 2 IT iterations, "
                       f"fftw_n_threads={threads} (FP64 FFTW-API shim; FFTW3 absent on this image)"}
+
+
+def reference_gpu_rate(iters: int = 200) -> dict | None:
+    """RT iterations/s of the reference's own GPU backend (GpuGrossPitaevskiSolver,
+    its kernels and FP64 cuFFT, oracle/_ref/libgpe_refgpu.so) on the workload."""
+    from oracle import oracle as O
+
+    if not os.path.exists(O.REFGPU_SO):
+        return None
+    cfg = O.default_config(nx=NX, ny=NY, nz=NZ, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
+                           pote_strategy="MEXICAN")
+    S = O.RefGpuSolver(cfg)
+    try:
+        S.imag_steps(20)
+        S.change_potential("MEXICAN_FREE")
+        S.real_steps(20, 0)  # warm-up (cuFFT plans exist since construction)
+        t0 = time.perf_counter()
+        S.real_steps(iters, 20)
+        dt = time.perf_counter() - t0
+    finally:
+        S.close()
+    return {"value": iters / dt, "unit": UNIT, "kind": "reference GPU backend (FP64 cuFFT, its CUDA kernels)",
+            "sample": f"{iters} RT iterations at {NX}x{NY}x{NZ} after 20 IT iterations, wall clock around a "
+                      f"device synchronisation"}
 
 
 def run_reference_arm(args):
@@ -386,9 +392,18 @@ def run_our_arm(args):
     per_gpu_rate = args.steps * ITERS_PER_STEP / (t_ms / 1e3)
     traffic = traffic_from_profiles(kname)
 
+    # the reference's own GPU backend (its CUDA kernels + FP64 cuFFT) on the same
+    # GPU, same workload: RT iterations after a short imaginary-time set-up
+    ref_gpu = None
+    if rank == 0 and ws == 1 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_rate()
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = reference_cpu_rate(args.cpu_budget)
+        # the reference's default fftw_n_threads (parameters.cpp:30) beside it
+        four = reference_cpu_rate(args.cpu_budget / 2, threads=4)
+        cpu["fftw_n_threads_4"] = {"value": four["value"], "sample": four["sample"]}
 
     if rank == 0:
         line = {
@@ -410,6 +425,7 @@ def run_our_arm(args):
             "kernels_ms": {k: round(v[0], 5) for k, v in kt.items()},
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(line), flush=True)
     solver.close()
@@ -471,8 +487,14 @@ def run_sweep(args):
     import gpesolver_b200 as G
     from gpesolver_b200 import sweep
 
+    from gpesolver_b200 import replicas
+
+    ws, rank, local = replicas.env()
+    replicas.init(ws, local, "nccl")
+    torch.cuda.set_device(local)
     iters = args.sweep_iters
-    js = sweep.sweep_json(count=args.sweep_members, seed=0, iter_imag=iters)
+    js_all = sweep.sweep_json(count=args.sweep_members, seed=0, iter_imag=iters)
+    js = replicas.shard(js_all, rank, ws)  # replicas: each GPU runs its own members
     ps = [G.params_from_json(j) for j in js]
     stream = torch.cuda.Stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -495,17 +517,21 @@ def run_sweep(args):
     stream.synchronize()
     launches0 = sum(m.launch_count() for m in b.members)
     times, e2e_times = [], []
-    with ClockSampler(0) as clk:
+    with ClockSampler(local) as clk:
         for _ in range(args.steps):
             with torch.cuda.stream(stream):
                 init_all()
                 flush.zero_()
+            stream.synchronize()
+            replicas.barrier(ws)
+            with torch.cuda.stream(stream):
                 e0, e1 = ev(), ev()
                 e0.record(stream)
                 b.imag_steps(iters)
                 e1.record(stream)
             stream.synchronize()
-            times.append(e0.elapsed_time(e1) / 1e3)
+            replicas.barrier(ws)
+            times.append(replicas.reduce(ws, e0.elapsed_time(e1) / 1e3, "max"))
     clocks = clk.summary()
     launches = (sum(m.launch_count() for m in b.members) - launches0) // args.steps
     # end to end: device-side initialisation, the solves, psi and energies to the host
@@ -527,7 +553,7 @@ def run_sweep(args):
 
     # the same members one after the other (each a fused single solve)
     seq = 0.0
-    for p in ps:
+    for p in (ps if ws == 1 else []):
         with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
             s.set_stream(stream.cuda_stream)
             with torch.cuda.stream(stream):
@@ -544,9 +570,9 @@ def run_sweep(args):
             seq += e0.elapsed_time(e1) / 1e3
 
     t = statistics.median(times)
-    counts = collections.Counter((j["nx"], j["ny"], j["nz"]) for j in js)
+    counts = collections.Counter((j["nx"], j["ny"], j["nz"]) for j in js_all)
     cpu = None
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and ws == 1:
         per = {g: reference_it_seconds(g, args.cpu_budget / len(counts)) for g in counts}
         cpu_sweep_s = sum(counts[g] * per[g][0] * iters for g in counts)
         cpu = {"value": len(ps) * iters / cpu_sweep_s, "unit": "member-iterations/s",
@@ -555,12 +581,15 @@ def run_sweep(args):
                          + " (the sweep time is these per-iteration times x members x iterations; "
                            "FP64 FFTW-API shim, FFTW3 absent)",
                "sweep_seconds": cpu_sweep_s}
+    replicas.finish(ws)
+    if rank != 0:
+        return
     line = {
-        "metric": SWEEP_METRIC, "value": len(ps) * iters / t, "unit": "member-iterations/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
+        "metric": SWEEP_METRIC, "value": len(js_all) * iters / t, "unit": "member-iterations/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
         "data": "synthetic (SplitMix64 seed 0 parameters; device-side CYLINDRICAL trap and GAUSS state)",
-        "config": {"workload": f"{len(ps)} imaginary-time solves x {iters} iterations, CYLINDRICAL, "
+        "config": {"workload": f"{len(js_all)} imaginary-time solves x {iters} iterations, CYLINDRICAL, "
                                f"GAUSS, edd~U[1.2,1.8], n_atoms~U[1e4,5e4], omega_r~U[40,80] Hz, "
                                f"omega_z/omega_r~U[1,4], dx=dy=120 nm, dz=600 nm",
                    "grids": {f"{g[0]}x{g[1]}x{g[2]}": c for g, c in sorted(counts.items())},
@@ -568,8 +597,9 @@ def run_sweep(args):
                    "schedule": "one CUDA graph per 64-iteration chunk, one branch per member",
                    "l2": "flushed before each timed sweep"},
         "sweep_seconds": t,
-        "sequential_gpu": {"value": len(ps) * iters / seq, "sweep_seconds": seq,
-                           "note": "the same members one after the other, each alone on the GPU"},
+        "sequential_gpu": ({"value": len(ps) * iters / seq, "sweep_seconds": seq,
+                            "note": "the same members one after the other, each alone on the GPU"}
+                           if seq > 0 else None),
         "e2e": {"value": len(ps) * iters / statistics.median(e2e_times), "unit": "member-iterations/s",
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
                 "note": "device-side initialisation, the solves, psi and energies of every member to the host"},
@@ -783,6 +813,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's GPU backend")
     ap.add_argument("--workload", default="rt", choices=["rt", "sweep", "accuracy", "warmstart"],
                     help="rt: the headline real-time benchmark; sweep: 64 batched imaginary-time solves")
     ap.add_argument("--sweep-members", type=int, default=64)

@@ -62,6 +62,7 @@ def build(ref: bool = True) -> None:
         targets.append("ref")
         if os.path.exists(os.path.join(os.path.dirname(HERE), "gpesolver_b200", "libgpe_b200.so")):
             targets.append("adapter")
+        targets.append("refgpu")
     subprocess.check_call(["make", "-s", "-C", HERE] + targets)
 
 
@@ -527,3 +528,59 @@ class AdapterSolver:
 
     def saved_energies(self) -> np.ndarray:
         return _saved_energies(self.L.gpeadp_saved_energies)
+
+
+# ---------------------------------------------------------------------------
+# The reference's GPU backend (cuFFT FP64), for timing beside this project
+# ---------------------------------------------------------------------------
+REFGPU_SO = os.path.join(HERE, "_ref", "libgpe_refgpu.so")
+_rglib = None
+
+
+def rglib():
+    global _rglib
+    if _rglib is None:
+        L = ctypes.CDLL(REFGPU_SO)
+        L.gperefgpu_create.argtypes = [ctypes.POINTER(RefConfig)]
+        L.gperefgpu_last_error.restype = ctypes.c_char_p
+        L.gperefgpu_imag_steps.argtypes = [ctypes.c_long]
+        L.gperefgpu_real_steps.argtypes = [ctypes.c_long, ctypes.c_long]
+        L.gperefgpu_change_potential.argtypes = [ctypes.c_char_p]
+        L.gperefgpu_export_psi.argtypes = [_dp]
+        L.gperefgpu_energy.argtypes = [_dp]
+        _rglib = L
+    return _rglib
+
+
+class RefGpuSolver:
+    """The reference's own GpuGrossPitaevskiSolver (its CUDA kernels and cuFFT
+    FP64), driven through its base-class iterations.  Needs a GPU."""
+
+    def __init__(self, cfg: dict):
+        L = rglib()
+        if L.gperefgpu_create(ctypes.byref(ref_config(cfg))) != 0:
+            raise RuntimeError(L.gperefgpu_last_error().decode())
+        self.n = cfg["nx"] * cfg["ny"] * cfg["nz"]
+
+    def close(self):
+        rglib().gperefgpu_destroy()
+
+    def imag_steps(self, k: int):
+        assert rglib().gperefgpu_imag_steps(k) == 0
+
+    def real_steps(self, k: int, first_iter: int = 0):
+        assert rglib().gperefgpu_real_steps(k, first_iter) == 0
+
+    def change_potential(self, key: str):
+        assert rglib().gperefgpu_change_potential(key.encode()) == 0
+
+    def psi(self) -> np.ndarray:
+        out = np.zeros(2 * self.n)
+        rglib().gperefgpu_export_psi(_ptr(out))
+        return out
+
+    def energy(self) -> np.ndarray:
+        out = np.zeros(6)
+        rglib().gperefgpu_energy(_ptr(out))
+        return out
+
