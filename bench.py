@@ -388,7 +388,9 @@ def run_our_arm(args):
     F = 8.0 * p.n
     R4 = 4.0 * p.n
     I = 8.0 * NX * 2 * NY * (NZ + 1)
-    b_rt = 6 * F + 3 * R4 + 4 * I  # algorithmic bytes per RT iteration (fused schedule)
+    # algorithmic bytes per RT iteration (fused schedule; 2F of them the
+    # real-space psi that the increment form keeps between phase steps)
+    b_rt = 8 * F + 3 * R4 + 4 * I
     per_gpu_rate = args.steps * ITERS_PER_STEP / (t_ms / 1e3)
     traffic = traffic_from_profiles(kname)
 

@@ -4,12 +4,13 @@
 // FFT lines along one axis with the elementwise physics fused into its loads
 // and stores:
 //
-//   X  pencils along x: kinetic  fwd FFT(nx) * exp(i(-dt/2m)k^2)/N * inv FFT(nx)
+//   X  pencils along x: kinetic  fwd FFT(nx) * (exp(i(-dt/2m)k^2) - 1)/N * inv FFT(nx)
 //                       dipolar  fwd FFT(2nx, upper half zero) * V_dd(k) * scale
 //                                * inv FFT(2nx), first nx kept
 //   Yi lines along y, inverse:   kinetic iFFT(ny); dipolar iFFT(2ny), first ny kept
 //   Z  rows along z:   dipolar C2R (pairs of rows packed in one complex FFT of
-//                      2nz) -> phi; kinetic iFFT(nz) -> psi; the real-time phases
+//                      2nz) -> phi; kinetic iFFT(nz) -> the kinetic increment,
+//                      added to the kept real-space psi (psi_r); the real-time phases
 //                      of two consecutive half steps merged into one rotation
 //                      (they see the same |psi|, V and phi); rho = w|psi|^2;
 //                      kinetic FFT(nz); dipolar R2C (pairs) -> spectrum
@@ -59,9 +60,15 @@ enum { ZM_RT_PRO = 0, ZM_RT_MID, ZM_RT_EPI, ZM_IT_PRO, ZM_IT_MID };
 // 128 bytes per line, coalesced), 8 for the 512-point dipolar lines.
 template <int L> constexpr int xy_count() { return L >= 512 ? 8 : 16; }
 
-// Kinetic x pencils: psi(x, ky, kz) -> FFT_x -> exp(i(-dt/2m)k^2) / N -> iFFT_x.
-// The forward transform ends and the inverse one starts in registers, with the
-// kinetic phase applied in between.
+// Kinetic x pencils, increment form: psi(x, ky, kz) -> FFT_x ->
+// (exp(i(-dt/2m)k^2) - 1) / N -> iFFT_x, i.e. the change the kinetic step makes
+// to psi, which the z / plane kernel adds to the real-space psi it kept from the
+// previous phase step (ZArgs::psi_r).  In exact arithmetic this is the kinetic
+// step itself; in FP32 the rounding of the transforms scales with |e^{i theta} -
+// 1| instead of with |psi|, so the per-step error is about one rounding of the
+// sum instead of that of a forward and an inverse 3D FFT.  The forward transform
+// ends and the inverse one starts in registers, with the factor applied in
+// between.
 template <class R, int NX, int CNT, int NT>
 __global__ void __launch_bounds__(NT)
     k3_x_kin(cplx<R> *__restrict__ psi, const cplx<R> *__restrict__ ex, const cplx<R> *__restrict__ ey,
@@ -97,7 +104,7 @@ __global__ void __launch_bounds__(NT)
             for (int q = 0; q < Fw::RL; ++q) {
                 const C wx = __ldg(&ex[Fw::last_index(tid, rd, q)]);
                 const C w  = cadd(cadd(wx, wyz), cmul(wx, wyz)); // (1+wx)(1+wyz) - 1
-                const C v  = apply_wm1(a[rd][q], w);
+                const C v  = cmul(a[rd][q], w);
                 a[rd][q]   = C{fma(v.x, inv_hi, v.x * inv_lo), fma(v.y, inv_hi, v.y * inv_lo)};
             }
         }
@@ -226,8 +233,9 @@ template <class R, int N, int CNT> struct YShape {
 // ---------------------------------------------------------------------------
 struct ZArgs {
     // fields
-    void *psi_in;        // kinetic spectrum (RT), or psi (RT_PRO, IT)
+    void *psi_in;        // RT: the kinetic increment's yz spectrum (psi in RT_PRO); IT: psi
     void *psi_out;       // RT: same as psi_in; IT: the next psi buffer
+    void *psi_r;         // RT: psi in real space after the last phase step (read, then rewritten)
     const void *bnd;     // IT: boundary values (last loaded psi)
     void *S;             // dipolar spectrum
     const void *V;
@@ -349,6 +357,7 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
             }
         }
         const R *Vg   = reinterpret_cast<const R *>(a.V);
+        C *pr         = reinterpret_cast<C *>(a.psi_r);
         const R hdt   = (R)a.half_dt, cdd = (R)a.cdd, wat = (R)a.w_atoms;
         for (int e = tid; e < RW * NZ; e += NT) {
             const int row = e / NZ, k = e % NZ;
@@ -357,6 +366,8 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
                 continue;
             const int i = rr / ny, j = rr - i * ny;
             C p         = kt[row + k * TK];
+            if (MODE != ZM_RT_PRO)
+                p = cadd(p, pr[(size_t)rr * NZ + k]); // psi + kinetic increment
             if (i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < NZ - 1) {
                 const R dens  = p.x * p.x + p.y * p.y;
                 const R am    = sqrt(dens);
@@ -365,8 +376,10 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
                 R s, c;
                 sincos_r<R>((R)-0.5 * hdt * total, &s, &c);
                 p = apply_wm1(p, C{(R)-2 * s * s, (R)2 * s * c});
-                kt[row + k * TK] = p;
             }
+            kt[row + k * TK] = p;
+            if (MODE != ZM_RT_EPI)
+                pr[(size_t)rr * NZ + k] = p;
             // rho for the next dipolar spectrum (stored in the phi tile)
             phis[row + k * TK] = wat * (p.x * p.x + p.y * p.y);
         }

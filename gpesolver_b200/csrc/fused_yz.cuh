@@ -5,10 +5,14 @@
 // pass.  k4_yz keeps one plane of each in shared memory and runs, for plane i,
 //
 //   dipolar  iFFT_y(2ny, lower half kept) -> C2R_z (row pairs) -> phi
-//   kinetic  iFFT_y(ny) -> iFFT_z(nz) -> phase -> FFT_z(nz) -> FFT_y(ny)
+//   kinetic  iFFT_y(ny) -> iFFT_z(nz) -> + psi_r -> phase -> FFT_z(nz) -> FFT_y(ny)
 //   dipolar  rho -> R2C_z (row pairs) -> FFT_y(2ny, upper half zero)
 //
-// (imaginary time: the Euler stencil step in place of the kinetic transforms),
+// (imaginary time: the Euler stencil step in place of the kinetic transforms).
+// In real time the x pass hands over the kinetic increment (fused.cuh,
+// k3_x_kin): its inverse yz transform is added to the real-space psi that the
+// previous plane kernel kept (psi_r, its own copy of the plane after the
+// phase step), and the new psi after the phase goes back to psi_r,
 // so one iteration is two kernels (x pass, yz plane) instead of four; the three
 // plane passes no longer go through global memory between each other.  The
 // z-line transforms pair through registers (iFFT_z ends, the phase is applied,
@@ -22,6 +26,8 @@
 //   DP  2nz x (ny/2 + 1): the row-pair lines of the real transforms; it shares
 //       the upper half of SP, which holds nothing between the pruned inverse y
 //       transform and the pruned forward one.
+//   RP   ny rows x PS  real-space psi of the previous phase step (real time,
+//       middle and last iterations)
 #pragma once
 
 #include "fused.cuh"
@@ -304,7 +310,12 @@ template <class R, int NY, int NZ> struct YZShape {
     static constexpr size_t PP_B = sizeof(C) * NY * PS;
     static constexpr size_t FP_B = sizeof(R) * NY * FS;
     static constexpr size_t DP_B = ALIAS ? 0 : sizeof(C) * LD * TD;
-    static constexpr size_t SMEM = SP_B + PP_B + FP_B + DP_B;
+    static constexpr size_t SMEM = SP_B + PP_B + FP_B + DP_B; // imaginary time, RT prologue
+    static constexpr size_t RP_B = sizeof(C) * NY * PS;
+    static constexpr size_t SMEM_RT = SMEM + RP_B;            // RT middle and last iterations
+    template <int MODE> static constexpr size_t smem() {
+        return (MODE == ZM_RT_MID || MODE == ZM_RT_EPI) ? SMEM_RT : SMEM;
+    }
     static constexpr int NT0     = 2 * NY * NZ / 16;
     static constexpr int NT      = NT0 < 128 ? 128 : (NT0 > 512 ? 512 : (NT0 + 31) / 32 * 32);
 };
@@ -401,15 +412,17 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     C *PP  = SP + 2 * NY * PS;
     R *FP  = reinterpret_cast<R *>(PP + NY * PS);
     C *DP  = G::ALIAS ? SP + NY * PS : reinterpret_cast<C *>(FP + NY * FS);
+    C *RP  = reinterpret_cast<C *>(g_smem + G::SMEM); // RT middle and last iterations only
     __shared__ double red[NT / 32];
 
     C *S_g         = reinterpret_cast<C *>(a.S) + (size_t)i * 2 * NY * NZ;
     const R *V_g   = reinterpret_cast<const R *>(a.V) + (size_t)i * NY * NZ;
     R *phi_g       = reinterpret_cast<R *>(a.phi) + (size_t)i * NY * NZ;
     C *P_o         = reinterpret_cast<C *>(a.psi_out) + (size_t)i * NY * NZ;
+    C *Pr_g        = reinterpret_cast<C *>(a.psi_r) + (size_t)i * NY * NZ;
     const R cdd    = (R)a.cdd;
 
-    // ---- load the planes (two cp.async groups: S; psi and V) -------------------
+    // ---- load the planes (cp.async groups: S; psi and V; kept real-space psi) ---
     if (HAS_INV)
         plane_in_async<C, 2 * NY, NZ, PS, NT>(SP, S_g, tid);
     cp_async_commit();
@@ -418,10 +431,17 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     if (MODE != ZM_IT_PRO)
         plane_in_async<R, NY, NZ, FS, NT>(FP, V_g, tid);
     cp_async_commit();
-    if (HAS_INV && !RT)
+    constexpr bool KEPT = MODE == ZM_RT_MID || MODE == ZM_RT_EPI;
+    if (KEPT) {
+        // needed only at the phase step: waited for there, behind the transforms
+        plane_in_async<C, NY, NZ, PS, NT>(RP, Pr_g, tid);
+        cp_async_commit();
+        cp_async_wait<1>();
+    } else if (HAS_INV && !RT) {
         cp_async_wait<1>(); // S; psi and V are waited for inside the dipolar inverse
-    else
+    } else {
         cp_async_wait<0>();
+    }
     __syncthreads();
 
     if constexpr (RT) {
@@ -503,6 +523,8 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                 FP[r * FS + k] += cdd * phi_g[e];
             }
         }
+        if (KEPT)
+            cp_async_wait<0>(); // RP, visible to the block after the barrier
         __syncthreads(); // FP = V + cdd phi
 
         // merged potential half steps: theta = -dt/2 [cV (V + cdd phi) + g3 |psi|^2 + gw |psi|^3]
@@ -537,10 +559,12 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
             return p;
         };
         if (MODE == ZM_RT_PRO) {
-            // psi is in real space
+            // psi is in real space; the plane after the phase is kept in psi_r
             for (int e = tid; e < NY * NZ; e += NT) {
                 const int r = e / NZ, k = e - r * NZ;
-                PP[r * PS + k] = phase(PP[r * PS + k], r, k);
+                const C v      = phase(PP[r * PS + k], r, k);
+                PP[r * PS + k] = v;
+                Pr_g[e]        = v;
             }
         } else {
 #pragma unroll
@@ -549,8 +573,14 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                     break;
                 const int y = ZI::Last::line(tid, rd);
 #pragma unroll
-                for (int q = 0; q < ZI::Last::RADIX; ++q)
-                    zr[rd][q] = phase(zr[rd][q], y, ZI::Last::elem(tid, rd, q));
+                for (int q = 0; q < ZI::Last::RADIX; ++q) {
+                    const int z = ZI::Last::elem(tid, rd, q);
+                    // psi = kept psi + kinetic increment, then the phase step;
+                    // the new psi goes back to RP (stored coalesced further on)
+                    zr[rd][q] = phase(cadd(zr[rd][q], RP[y * PS + z]), y, z);
+                    if (MODE == ZM_RT_MID)
+                        RP[y * PS + z] = zr[rd][q];
+                }
             }
             if (MODE == ZM_RT_EPI) {
                 // psi in real space -> global (the last z reads of PP are behind a barrier)
@@ -581,6 +611,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
             }
             ZF::First::write(PP, zr, tid);
             __syncthreads();
+            plane_out<R, NY, NZ, PS, NT>(Pr_g, RP, tid); // kept psi for the next iteration
             joint_stages<R2C, 0, R2C::NSTG, ZF, 1, ZF::NSTG>(DP, dzt, dzl, PP, kzt, kzl, tid);
         }
         // R2C unpacking -> SP rows < ny || kinetic FFT_y stage 0

@@ -249,6 +249,7 @@ template <class R> class Solver final : public SolverBase {
                 fused_dim_xy(ny) && fused_dim_z(nz);
         if (fused) {
             S2.alloc((size_t)nx * 2 * ny * nz);
+            psir.alloc(N);
             zpartial.alloc((size_t)(nx * ny + 31) / 32);
             ticket.alloc(1);
             build_vk2();
@@ -711,9 +712,10 @@ template <class R> class Solver final : public SolverBase {
                     b = 2 * S2h + (double)sizeof(R) * (nx + 1) * (ny + 1) * nz; // + the V_dd table
                 } else if (which == GPE_K_F_YZ) {
                     f_yz<ZM_RT_MID>(cur, psi.p, psi.p, coef_dev.p, 0);
-                    // psi R+W, spectrum (2ny rows) R+W, V read (phi is written
-                    // only by the last iteration of a call)
-                    b = 2 * F + 2 * S2b + Rb;
+                    // kinetic increment R+W, real-space psi R+W, spectrum (2ny
+                    // rows) R+W, V read (phi is written only by the last
+                    // iteration of a call)
+                    b = 4 * F + 2 * S2b + Rb;
                 } else if (which == GPE_K_F_X) {
                     f_x(cur, true, nullptr);
                     b = 2 * F + 2 * S2h; // kinetic R+W; dipolar reads and writes nx of 2nx planes
@@ -725,7 +727,8 @@ template <class R> class Solver final : public SolverBase {
                     b = 2 * F + S2h + S2b;
                 } else {
                     f_z<ZM_RT_MID>(cur, psi.p, psi.p, coef_dev.p, 0);
-                    b = 2 * F + 2 * S2h + Rb + Rb; // psi R+W, spectrum R+W, V read, phi write
+                    // increment R+W, real-space psi R+W, spectrum R+W, V read, phi write
+                    b = 4 * F + 2 * S2h + Rb + Rb;
                 }
                 break;
             }
@@ -821,11 +824,11 @@ template <class R> class Solver final : public SolverBase {
 #define GPE_SETYZ(A, B)                                                                            \
     if (ny == A && nz == B) {                                                                      \
         using G = YZShape<R, A, B>;                                                                \
-        set((const void *)k4_yz<R, A, B, ZM_RT_PRO>, G::SMEM);                                     \
-        set((const void *)k4_yz<R, A, B, ZM_RT_MID>, G::SMEM);                                     \
-        set((const void *)k4_yz<R, A, B, ZM_RT_EPI>, G::SMEM);                                     \
-        set((const void *)k4_yz<R, A, B, ZM_IT_PRO>, G::SMEM);                                     \
-        set((const void *)k4_yz<R, A, B, ZM_IT_MID>, G::SMEM);                                     \
+        set((const void *)k4_yz<R, A, B, ZM_RT_PRO>, G::template smem<ZM_RT_PRO>());               \
+        set((const void *)k4_yz<R, A, B, ZM_RT_MID>, G::template smem<ZM_RT_MID>());               \
+        set((const void *)k4_yz<R, A, B, ZM_RT_EPI>, G::template smem<ZM_RT_EPI>());               \
+        set((const void *)k4_yz<R, A, B, ZM_IT_PRO>, G::template smem<ZM_IT_PRO>());               \
+        set((const void *)k4_yz<R, A, B, ZM_IT_MID>, G::template smem<ZM_IT_MID>());               \
     }
             GPE_YZ_CASES(GPE_SETYZ)
 #undef GPE_SETYZ
@@ -888,6 +891,7 @@ template <class R> class Solver final : public SolverBase {
         ZArgs a{};
         a.psi_in     = pin;
         a.psi_out    = pout;
+        a.psi_r      = psir.p;
         a.bnd        = bnd.p;
         a.S          = S2.p;
         a.V          = V.p;
@@ -938,7 +942,7 @@ template <class R> class Solver final : public SolverBase {
 #define GPE_LYZ(A, B)                                                                              \
     if (ny == A && nz == B) {                                                                      \
         using G = YZShape<R, A, B>;                                                                \
-        launch(k4_yz<R, A, B, MODE>, nx, G::NT, G::SMEM, s, a, t);                                \
+        launch(k4_yz<R, A, B, MODE>, nx, G::NT, G::template smem<MODE>(), s, a, t);               \
     }
             GPE_YZ_CASES(GPE_LYZ)
 #undef GPE_LYZ
@@ -1112,6 +1116,7 @@ template <class R> class Solver final : public SolverBase {
     // fused pipeline (compile-time line lengths; complex64 only)
     bool fused = false;
     DevBuf<C> S2;
+    DevBuf<C> psir; // real time: psi in real space after the last phase step
     DevBuf<R> vk2;
     DevBuf<double> zpartial;
     DevBuf<unsigned> ticket;
