@@ -364,3 +364,29 @@ def test_energy_history_equals_per_check_energies():
             want.append(b.calc_energy().e_total)
         np.testing.assert_array_equal(hist, want)
         np.testing.assert_array_equal(a.export_data(), b.export_data())
+
+
+@pytest.mark.parametrize("dims", [(64, 64, 16), (32, 256, 16)])
+def test_increment_form_keeps_long_real_time_runs_close_to_fp64(dims):
+    # 3000 RT iterations: the fused schedules (the plane kernel at 64^2 x 16,
+    # the four-kernel pipeline at 32 x 256 x 16) apply the kinetic step as
+    # psi + iFFT[(e^{i theta} - 1) FFT psi]; the split schedule applies
+    # iFFT[e^{i theta} FFT psi], whose FP32 rounding scales with |psi|
+    nx, ny, nz = dims
+    cfg = O.default_config(nx=nx, ny=ny, nz=nz, init_strategy="GAUSS", pote_strategy="HARMONIC",
+                           dx=200.0, dy=200.0, dz=800.0, edd=None, edd_start=0.70, edd_stop=0.80,
+                           iter_real=3000)
+    p = gparams(cfg)
+    V, psi0 = G.potential(p), G.initial_psi(p)
+    psis = {}
+    for name, prec, sched in (("fp64", "c128", "split"), ("fused", "c64", "auto"), ("split", "c64", "split")):
+        with G.B200GrossPitaevskiSolver(p, precision=prec, schedule=sched) as s:
+            s.load_pote(V)
+            s.load_buffer(psi0)
+            s.imag_steps(100)
+            s.real_steps(3000, 0)
+            psis[name] = s.export_data()
+    e_fused = rel_l2(psis["fused"], psis["fp64"])
+    e_split = rel_l2(psis["split"], psis["fp64"])
+    assert e_fused < 1e-5
+    assert e_fused < 0.5 * e_split, (e_fused, e_split)
