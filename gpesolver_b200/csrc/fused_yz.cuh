@@ -28,6 +28,7 @@
 //       transform and the pruned forward one.
 //   RP   ny rows x PS  real-space psi of the previous phase step (real time,
 //       middle and last iterations)
+//   XM, XP  ny rows x PS each: psi of planes i - 1 and i + 1 (imaginary time)
 #pragma once
 
 #include "fused.cuh"
@@ -313,8 +314,9 @@ template <class R, int NY, int NZ> struct YZShape {
     static constexpr size_t SMEM = SP_B + PP_B + FP_B + DP_B; // imaginary time, RT prologue
     static constexpr size_t RP_B = sizeof(C) * NY * PS;
     static constexpr size_t SMEM_RT = SMEM + RP_B;            // RT middle and last iterations
+    static constexpr size_t SMEM_IT = SMEM + 2 * RP_B;        // IT: the two x-neighbour planes
     template <int MODE> static constexpr size_t smem() {
-        return (MODE == ZM_RT_MID || MODE == ZM_RT_EPI) ? SMEM_RT : SMEM;
+        return (MODE == ZM_RT_MID || MODE == ZM_RT_EPI) ? SMEM_RT : (MODE == ZM_IT_MID ? SMEM_IT : SMEM);
     }
     static constexpr int NT0     = 2 * NY * NZ / 16;
     static constexpr int NT      = NT0 < 128 ? 128 : (NT0 > 512 ? 512 : (NT0 + 31) / 32 * 32);
@@ -413,6 +415,8 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     R *FP  = reinterpret_cast<R *>(PP + NY * PS);
     C *DP  = G::ALIAS ? SP + NY * PS : reinterpret_cast<C *>(FP + NY * FS);
     C *RP  = reinterpret_cast<C *>(g_smem + G::SMEM); // RT middle and last iterations only
+    C *XM  = RP;                                      // IT: x-neighbour planes
+    C *XP  = RP + NY * PS;
     __shared__ double red[NT / 32];
 
     C *S_g         = reinterpret_cast<C *>(a.S) + (size_t)i * 2 * NY * NZ;
@@ -430,6 +434,11 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
         plane_in_async<C, NY, NZ, PS, NT>(PP, reinterpret_cast<const C *>(a.psi_in) + (size_t)i * NY * NZ, tid);
     if (MODE != ZM_IT_PRO)
         plane_in_async<R, NY, NZ, FS, NT>(FP, V_g, tid);
+    if (MODE == ZM_IT_MID && i >= 1 && i < nx - 1) {
+        const C *pin = reinterpret_cast<const C *>(a.psi_in);
+        plane_in_async<C, NY, NZ, PS, NT>(XM, pin + (size_t)(i - 1) * NY * NZ, tid);
+        plane_in_async<C, NY, NZ, PS, NT>(XP, pin + (size_t)(i + 1) * NY * NZ, tid);
+    }
     cp_async_commit();
     constexpr bool KEPT = MODE == ZM_RT_MID || MODE == ZM_RT_EPI;
     if (KEPT) {
@@ -696,9 +705,9 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                 if (!xin || r < 1 || r >= NY - 1 || k < 1 || k >= NZ - 1) {
                     o = __ldg(&bnd[q]);
                 } else {
-                    const C *pp = PP + r * PS + k; // this plane (shared), x neighbours (global)
+                    const C *pp = PP + r * PS + k; // this plane and its x neighbours (shared)
                     const C c0 = cscale(pp[0], sc);
-                    const C xm = cscale(__ldg(&pin[q - pln]), sc), xp = cscale(__ldg(&pin[q + pln]), sc);
+                    const C xm = cscale(XM[r * PS + k], sc), xp = cscale(XP[r * PS + k], sc);
                     const C ym = cscale(pp[-PS], sc), yp = cscale(pp[PS], sc);
                     const C zm = cscale(pp[-1], sc), zp = cscale(pp[1], sc);
                     const R vv   = FP[r * FS + k];
