@@ -477,6 +477,93 @@ def reference_it_seconds(grid, budget_s: float) -> tuple[float, int]:
     return dt / n, n
 
 
+def run_imag(args):
+    """Imaginary-time iterations/s (the reference's imag_time_iter: dipolar phi,
+    Euler update, norm, normalisation) at config 1 (64^2 x 16, HARMONIC, GAUSS)
+    and at 128^2 x 32 (the README run's IT phase), one JSON line per grid, with
+    the whole iteration against B_IT = 2F + 3R + 4I and the reference's CPU
+    code timed beside it."""
+    import numpy as np
+    import torch
+
+    import gpesolver_b200 as G
+
+    torch.cuda.set_device(0)
+    peak, peak_kind = measured_peak()
+    cases = [("config 1: imaginary time, 64x64x16, HARMONIC (60, 60, 120) Hz, GAUSS, edd=1.5, n_atoms=2e4",
+              dict(workload_json("IT"), nx=64, ny=64, nz=16, pote_strategy="HARMONIC", init_strategy="GAUSS")),
+             ("imaginary-time phase of the README run, 128x128x32, MEXICAN(dd=1500 nm), MULTIPLE_GAUSS(2)",
+              workload_json("IT"))]
+    for desc, j in cases:
+        p = G.params_from_json(j)
+        s = G.B200GrossPitaevskiSolver(p, precision="c64")
+        stream = torch.cuda.Stream()
+        s.set_stream(stream.cuda_stream)
+        s.init_pote()
+        s.init_buffer()
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                s.imag_steps(ITERS_PER_STEP)
+        stream.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        l0 = s.launch_count()
+        with ClockSampler(0) as clk:
+            with torch.cuda.stream(stream):
+                for e0, e1 in evs:
+                    flush.zero_()
+                    e0.record(stream)
+                    s.imag_steps(ITERS_PER_STEP)
+                    e1.record(stream)
+            stream.synchronize()
+        launches = s.launch_count() - l0
+        t_ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+        value = args.steps * ITERS_PER_STEP / (t_ms / 1e3)
+        e = s.calc_energy().e_total
+        s.close()
+        F, R4 = 8.0 * p.nx * p.ny * p.nz, 4.0 * p.nx * p.ny * p.nz
+        I = 8.0 * p.nx * 2 * p.ny * (p.nz + 1)
+        b_it = 2 * F + 3 * R4 + 4 * I
+        cpu = None
+        if not args.no_cpu_baseline:
+            sec, n = reference_it_seconds_cfg(j, args.cpu_budget)
+            cpu = {"value": 1.0 / sec, "unit": "iterations/s", "cores": os.cpu_count() or 1,
+                   "kind": "reference", "sample": f"{n} IT iterations at {p.nx}x{p.ny}x{p.nz}, "
+                   f"fftw_n_threads={os.cpu_count() or 1} (FP64 FFTW-API shim; FFTW3 absent on this image)"}
+        print(json.dumps({
+            "metric": f"imaginary-time iterations/s at {p.nx}x{p.ny}x{p.nz}", "value": value,
+            "unit": "iterations/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic (reference initializers, deterministic)",
+            "config": {"workload": desc, "grid": [p.nx, p.ny, p.nz], "iterations_per_step": ITERS_PER_STEP,
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "gpu_launches": launches,
+            "roofline_step": {"algorithmic_bytes_per_iteration": b_it, "achieved": b_it * value / 1e9,
+                              "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                              "frac": b_it * value / 1e9 / peak},
+            "energy_after": e, "clocks": clk.summary(), "cpu_baseline": cpu}), flush=True)
+
+
+def reference_it_seconds_cfg(j: dict, budget_s: float) -> tuple[float, int]:
+    """Seconds per imaginary-time iteration of the reference's CPU solver on the
+    configuration j (a gpe_params.json dict), from a bounded sample."""
+    from oracle import oracle as O
+
+    keys = ("nx", "ny", "nz", "dx", "dy", "dz", "m", "n_atoms", "omega_x", "omega_y", "omega_z", "dd",
+            "edd", "init_strategy", "initial_maximas", "pote_strategy")
+    cfg = O.default_config(**{k: j[k] for k in keys if k in j}, fftw_n_threads=os.cpu_count() or 1)
+    S = O.RefSolver(cfg) if O.ref_available() else O.OracleSolver(cfg)
+    S.imag_steps(1)
+    n, t0 = 0, time.perf_counter()
+    while n < 2 or (time.perf_counter() - t0 < budget_s and n < 500):
+        S.imag_steps(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    S.close()
+    return dt / n, n
+
+
 def run_sweep(args):
     """64 imaginary-time ground states with seeded parameters (SplitMix64, seed
     0) over mixed grids, as one B200Batch, against the same members run one
@@ -816,8 +903,9 @@ def main():
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's GPU backend")
-    ap.add_argument("--workload", default="rt", choices=["rt", "sweep", "accuracy", "warmstart"],
-                    help="rt: the headline real-time benchmark; sweep: 64 batched imaginary-time solves")
+    ap.add_argument("--workload", default="rt", choices=["rt", "imag", "sweep", "accuracy", "warmstart"],
+                    help="rt: the headline real-time benchmark; imag: imaginary-time iterations/s; "
+                         "sweep: 64 batched imaginary-time solves")
     ap.add_argument("--sweep-members", type=int, default=64)
     ap.add_argument("--sweep-iters", type=int, default=1000)
     ap.add_argument("--ws-train", type=int, default=2000)
@@ -838,6 +926,8 @@ def main():
         args.warmup = 3
     if args.workload == "sweep":
         run_sweep(args)
+    elif args.workload == "imag":
+        run_imag(args)
     elif args.workload == "accuracy":
         run_accuracy(args)
     elif args.workload == "warmstart":
