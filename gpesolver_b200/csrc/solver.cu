@@ -250,6 +250,7 @@ template <class R> class Solver final : public SolverBase {
         if (fused) {
             S2.alloc((size_t)nx * 2 * ny * nz);
             psir.alloc(N);
+            GPE_CUDA(cudaMemsetAsync(psir.p, 0, sizeof(C) * N, cur)); // defined before any RT call
             zpartial.alloc((size_t)(nx * ny + 31) / 32);
             ticket.alloc(1);
             build_vk2();

@@ -2,8 +2,8 @@
 // parameters (edd, n_atoms, omega_r, omega_z) to a ground-state amplitude
 // |psi_0| on the solver grid; imaginary time then refines that guess instead of
 // starting from a Gaussian.  The reference has no counterpart (it always starts
-// from its initialisers); plain Gaussian-start imaginary time stays the judge
-// of the prediction.
+// from its initialisers); plain Gaussian-start imaginary time stays the
+// fallback and the reference answer the prediction is measured against.
 //
 // Network (weights BF16, arithmetic FP32):
 //   dense 4 -> H, SiLU;  dense H -> C0 * X0 * Y0 * Z0 (the latent volume), SiLU
