@@ -22,7 +22,7 @@
 // conflict-free for both the y columns and the z rows):
 //   SP  2ny rows x PS  dipolar plane (ky or y, kz - 1)
 //   PP   ny rows x PS  psi plane (ky or y, kz or z)            (real time)
-//   FP   ny rows x (nz+1) reals: V + cdd phi, then rho
+//   FP   ny rows x (nz+1) reals: V + cdd phi, then rho (even rows, then odd rows)
 //   DP  2nz x (ny/2 + 1): the row-pair lines of the real transforms; it shares
 //       the upper half of SP, which holds nothing between the pruned inverse y
 //       transform and the pruned forward one.
@@ -309,7 +309,13 @@ template <class R, int NY, int NZ> struct YZShape {
     static constexpr bool ALIAS  = LD * TD <= NY * PS; // DP fits in the upper half of SP
     static constexpr size_t SP_B = sizeof(C) * 2 * NY * PS;
     static constexpr size_t PP_B = sizeof(C) * NY * PS;
-    static constexpr size_t FP_B = sizeof(R) * NY * FS;
+    // FP keeps even rows and odd rows in two halves, the odd half starting 16
+    // banks further on: lanes of consecutive rows, and lanes of consecutive row
+    // pairs, then fall in distinct banks (FS odd)
+    static constexpr int FH      = NP * FS + (((16 - (NP * FS) % 32) % 32) + 32) % 32;
+    static constexpr int FPN     = FH + NP * FS;     // floats in FP
+    static constexpr size_t FP_B = sizeof(R) * FPN;
+    static __device__ __forceinline__ int fpi(int r, int k) { return (r & 1) * FH + (r >> 1) * FS + k; }
     static constexpr size_t DP_B = ALIAS ? 0 : sizeof(C) * LD * TD;
     static constexpr size_t SMEM = SP_B + PP_B + FP_B + DP_B; // imaginary time, RT prologue
     static constexpr size_t RP_B = sizeof(C) * NY * PS;
@@ -340,9 +346,10 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
         cp_async_wait<0>(); // visible to the block after the next barrier
         // pair lines: z[m] = X_a[m] + i X_b[m] over the full 2nz-point spectrum
         // (bins 1..nz stored at kz - 1, bin 0 is zero, bins > nz by symmetry);
-        // DP may share SP's upper half (rows >= NY), which nothing reads any more
+        // DP may share SP's upper half (rows >= NY), which nothing reads any more.
+        // Consecutive threads take consecutive m: SP rows read contiguously.
         for (int e = t; e < NP * LD; e += NTG) {
-            const int p = e % NP, m = e / NP;
+            const int m = e % LD, p = e / LD;
             C z         = C{(R)0, (R)0};
             if (m > 0) {
                 const int mm = m <= NZ ? m : LD - m;
@@ -366,7 +373,7 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
             const R f   = (r & 1) ? zz.y : zz.x;
             if (WRITE_PHI)
                 phi_g[e] = f;
-            FP[r * FS + k] += cdd * f;
+            FP[G::fpi(r, k)] += cdd * f;
         }
     }
 
@@ -374,8 +381,8 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
     // FP must be complete (caller synchronised).
     static __device__ __forceinline__ void forward(C *SP, C *DP, const R *FP, C *S_g, const YZTwid &tw, int t) {
         for (int e = t; e < NP * NZ; e += NTG) {
-            const int p = e % NP, m = e / NP;
-            DP[p + m * TD] = C{FP[(2 * p) * FS + m], FP[(2 * p + 1) * FS + m]};
+            const int m = e % NZ, p = e / NZ;
+            DP[p + m * TD] = C{FP[G::fpi(2 * p, m)], FP[G::fpi(2 * p + 1, m)]};
         }
         group_sync<BAR, NTG>();
         PlanePass<-1, R, LD, NP, 1, TD, NTG, false, false, true, false, BAR>::run(DP, (const C *)tw.dz.tw,
@@ -413,7 +420,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     C *SP  = reinterpret_cast<C *>(g_smem);
     C *PP  = SP + 2 * NY * PS;
     R *FP  = reinterpret_cast<R *>(PP + NY * PS);
-    C *DP  = G::ALIAS ? SP + NY * PS : reinterpret_cast<C *>(FP + NY * FS);
+    C *DP  = G::ALIAS ? SP + NY * PS : reinterpret_cast<C *>(FP + G::FPN);
     C *RP  = reinterpret_cast<C *>(g_smem + G::SMEM); // RT middle and last iterations only
     C *XM  = RP;                                      // IT: x-neighbour planes
     C *XP  = RP + NY * PS;
@@ -432,8 +439,13 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     cp_async_commit();
     if (RT || MODE == ZM_IT_MID)
         plane_in_async<C, NY, NZ, PS, NT>(PP, reinterpret_cast<const C *>(a.psi_in) + (size_t)i * NY * NZ, tid);
-    if (MODE != ZM_IT_PRO)
-        plane_in_async<R, NY, NZ, FS, NT>(FP, V_g, tid);
+    if (MODE != ZM_IT_PRO) {
+#pragma unroll 4
+        for (int e = tid; e < NY * NZ; e += NT) {
+            const int r = e / NZ, k = e - r * NZ;
+            cp_async4(&FP[G::fpi(r, k)], &V_g[e]);
+        }
+    }
     if (MODE == ZM_IT_MID && i >= 1 && i < nx - 1) {
         const C *pin = reinterpret_cast<const C *>(a.psi_in);
         plane_in_async<C, NY, NZ, PS, NT>(XM, pin + (size_t)(i - 1) * NY * NZ, tid);
@@ -480,9 +492,10 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
             joint_stages<DYI, 0, DYI::NSTG, KYI, 0, KYI::NSTG>(SP, dyt, dyl, PP, kyt, kyl, tid);
             // C2R pair lines: z[m] = X_a[m] + i X_b[m] over the full 2nz-point
             // spectrum (bins 1..nz stored at kz - 1, bin 0 zero, bins > nz by
-            // symmetry); DP shares SP's upper half, which holds nothing now
+            // symmetry); DP shares SP's upper half, which holds nothing now;
+            // consecutive threads take consecutive m (SP rows read contiguously)
             for (int e = tid; e < NP * LD; e += NT) {
-                const int p = e % NP, m = e / NP;
+                const int m = e % LD, p = e / LD;
                 C z         = C{(R)0, (R)0};
                 if (m > 0) {
                     const int mm = m <= NZ ? m : LD - m;
@@ -516,8 +529,8 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                             continue;
                         const int k = C2R::Last::elem(tid, rd, q);
                         const C v   = ca[rd][q];
-                        FP[(2 * p) * FS + k] += cdd * v.x;
-                        FP[(2 * p + 1) * FS + k] += cdd * v.y;
+                        FP[G::fpi(2 * p, k)] += cdd * v.x;
+                        FP[G::fpi(2 * p + 1, k)] += cdd * v.y;
                         if (WRITE_PHI) {
                             phi_g[(2 * p) * NZ + k]     = v.x;
                             phi_g[(2 * p + 1) * NZ + k] = v.y;
@@ -529,7 +542,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
             // prologue: phi of the previous calc_fi3d
             for (int e = tid; e < NY * NZ; e += NT) {
                 const int r = e / NZ, k = e - r * NZ;
-                FP[r * FS + k] += cdd * phi_g[e];
+                FP[G::fpi(r, k)] += cdd * phi_g[e];
             }
         }
         if (KEPT)
@@ -555,7 +568,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
         const R hdt = (R)a.half_dt, wat = (R)a.w_atoms;
         const bool xin = i >= 1 && i < nx - 1;
         auto phase = [&](C p, int y, int z) -> C {
-            const int f = y * FS + z;
+            const int f = G::fpi(y, z);
             if (xin && y >= 1 && y < NY - 1 && z >= 1 && z < NZ - 1) {
                 const R dens  = p.x * p.x + p.y * p.y;
                 const R am    = sqrt(dens);
@@ -603,8 +616,8 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
 
         // R2C pair lines from rho (upper half zero) || kinetic FFT_z
         for (int e = tid; e < NP * NZ; e += NT) {
-            const int p = e % NP, m = e / NP;
-            DP[p + m * TD] = C{FP[(2 * p) * FS + m], FP[(2 * p + 1) * FS + m]};
+            const int m = e % NZ, p = e / NZ;
+            DP[p + m * TD] = C{FP[G::fpi(2 * p, m)], FP[G::fpi(2 * p + 1, m)]};
         }
         if (MODE == ZM_RT_PRO) {
             __syncthreads();
@@ -688,7 +701,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
             for (int e = tid; e < NY * NZ; e += NT) {
                 const int r = e / NZ, k = e - r * NZ;
                 const C p   = __ldg(&pin[base + e]);
-                FP[r * FS + k] = wat * (p.x * p.x + p.y * p.y);
+                FP[G::fpi(r, k)] = wat * (p.x * p.x + p.y * p.y);
             }
         } else {
             DW::template inverse<true>(SP, DP, FP, phi_g, cdd, tw, tid);
@@ -710,7 +723,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                     const C xm = cscale(XM[r * PS + k], sc), xp = cscale(XP[r * PS + k], sc);
                     const C ym = cscale(pp[-PS], sc), yp = cscale(pp[PS], sc);
                     const C zm = cscale(pp[-1], sc), zp = cscale(pp[1], sc);
-                    const R vv   = FP[r * FS + k];
+                    const R vv   = FP[G::fpi(r, k)];
                     const R dens = c0.x * c0.x + c0.y * c0.y;
                     const R am   = sqrt(dens);
                     const R nl   = g3w * dens + gw15 * (am * am * am);
@@ -722,7 +735,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                 }
                 pout[q] = o;
                 acc += (double)o.x * o.x + (double)o.y * o.y;
-                FP[r * FS + k] = wat * (o.x * o.x + o.y * o.y);
+                FP[G::fpi(r, k)] = wat * (o.x * o.x + o.y * o.y);
             }
         }
         __syncthreads(); // rho complete; SP's upper half (DP) free
