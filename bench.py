@@ -479,10 +479,10 @@ def reference_it_seconds(grid, budget_s: float) -> tuple[float, int]:
 
 def run_imag(args):
     """Imaginary-time iterations/s (the reference's imag_time_iter: dipolar phi,
-    Euler update, norm, normalisation) at config 1 (64^2 x 16, HARMONIC, GAUSS)
-    and at 128^2 x 32 (the README run's IT phase), one JSON line per grid, with
-    the whole iteration against B_IT = 2F + 3R + 4I and the reference's CPU
-    code timed beside it."""
+    Euler update, norm, normalisation) for the plain imaginary-time run (64^2 x
+    16, HARMONIC, GAUSS) and at 128^2 x 32 (the README run's IT phase), one JSON
+    line per grid, with the whole iteration against B_IT = 2F + 3R + 4I and the
+    reference's CPU code timed beside it."""
     import numpy as np
     import torch
 
@@ -490,7 +490,7 @@ def run_imag(args):
 
     torch.cuda.set_device(0)
     peak, peak_kind = measured_peak()
-    cases = [("config 1: imaginary time, 64x64x16, HARMONIC (60, 60, 120) Hz, GAUSS, edd=1.5, n_atoms=2e4",
+    cases = [("plain imaginary-time run, 64x64x16, HARMONIC (60, 60, 120) Hz, GAUSS, edd=1.5, n_atoms=2e4",
               dict(workload_json("IT"), nx=64, ny=64, nz=16, pote_strategy="HARMONIC", init_strategy="GAUSS")),
              ("imaginary-time phase of the README run, 128x128x32, MEXICAN(dd=1500 nm), MULTIPLE_GAUSS(2)",
               workload_json("IT"))]

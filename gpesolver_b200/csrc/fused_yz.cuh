@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     using C                = cplx<R>;
     using G                = YZShape<R, NY, NZ>;
     constexpr int NT       = G::NT;
-    constexpr int PS = G::PS, FS = G::FS;
+    constexpr int PS       = G::PS;
     constexpr bool RT      = MODE <= ZM_RT_EPI;
     constexpr bool HAS_INV = (MODE == ZM_RT_MID || MODE == ZM_RT_EPI || MODE == ZM_IT_MID);
     const int tid          = threadIdx.x;

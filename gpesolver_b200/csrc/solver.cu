@@ -504,7 +504,8 @@ template <class R> class Solver final : public SolverBase {
             if (!lazy)
                 set_divisor_one();
             if (fused) {
-                fused_imag(k);
+                // the energy kernels between checks only read psi: one prologue
+                fused_imag(k, c == 0);
             } else {
                 long done = 0;
                 while (k - done >= kItChunk) {
@@ -1087,8 +1088,12 @@ template <class R> class Solver final : public SolverBase {
         run_fused_graph(12, (int)(mid - done));
     }
 
-    void fused_imag(long k) {
-        run_fused_graph(20, 0);
+    // prologue = false: the dipolar spectrum is already that of the stored psi
+    // (the previous call ended with an IT iteration and nothing has written psi
+    // since); the prologue would recompute it bit for bit.
+    void fused_imag(long k, bool prologue = true) {
+        if (prologue)
+            run_fused_graph(20, 0);
         const int CH = kItChunk;
         long done    = 0;
         while (k - done >= CH) {

@@ -169,7 +169,7 @@ def test_short_runs_match_oracle_with_edd_ramp(k):
 
 
 def test_readme_config_imaginary_time_c64():
-    # BASELINE config 1 geometry (64^2 x 16, HARMONIC, GAUSS), 200 IT iterations
+    # the plain imaginary-time run's geometry (64^2 x 16, HARMONIC, GAUSS), 200 IT iterations
     cfg = O.default_config(nx=64, ny=64, nz=16, init_strategy="GAUSS", pote_strategy="HARMONIC")
     p = gparams(cfg, "IT")
     ref = O.OracleSolver(cfg)
@@ -188,7 +188,7 @@ def test_readme_config_imaginary_time_c64():
 
 
 def test_full_simulation_128_c64():
-    # BASELINE config 2 geometry (128^2 x 32, MEXICAN, 2 maxima), short FS run
+    # the README full simulation's geometry (128^2 x 32, MEXICAN, 2 maxima), short FS run
     cfg = O.default_config(nx=128, ny=128, nz=32, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
                            pote_strategy="MEXICAN", fftw_n_threads=8)
     p = gparams(cfg)
@@ -209,7 +209,7 @@ def test_full_simulation_128_c64():
 
 
 def test_real_time_conserves_norm_at_256():
-    # BASELINE config 3 geometry (256^2 x 64, FREE, SETUP_GAUSS 3x3x2, edd ramp):
+    # the 256^2 x 64 ramp study's geometry (FREE, SETUP_GAUSS 3x3x2, edd ramp):
     # size-independent property -- split-step RT is unitary, the norm stays 1.
     cfg = O.default_config(nx=256, ny=256, nz=64, init_strategy="SETUP_GAUSS", bec_droplets_x=3,
                            bec_droplets_y=3, bec_droplets_z=2, pote_strategy="FREE", edd=None,
@@ -348,19 +348,21 @@ def test_real_steps_after_coefficient_buffer_grows():
     assert rel_l2(out[0], out[1]) < 1e-5
 
 
-def test_energy_history_equals_per_check_energies():
+@pytest.mark.parametrize("dims,k", [((32, 32, 16), 10), ((32, 256, 16), 7)])
+def test_energy_history_equals_per_check_energies(dims, k):
     """imag_steps_energies keeps the energies on the device between host
-    synchronisations: the same numbers as stepping and calling calc_energy."""
-    cfg = WELL_CONDITIONED(32, 32, 16)
+    synchronisations (and rebuilds the dipolar spectrum only at its start):
+    bit for bit the numbers of stepping and calling calc_energy."""
+    cfg = WELL_CONDITIONED(*dims)
     p = gparams(cfg)
     with G.B200GrossPitaevskiSolver(p) as a, G.B200GrossPitaevskiSolver(p) as b:
         for s in (a, b):
             s.load_pote(G.potential(p))
             s.load_buffer(G.initial_psi(p))
-        hist = a.imag_steps_energies(10, 6)
+        hist = a.imag_steps_energies(k, 6)
         want = []
         for _ in range(6):
-            b.imag_steps(10)
+            b.imag_steps(k)
             want.append(b.calc_energy().e_total)
         np.testing.assert_array_equal(hist, want)
         np.testing.assert_array_equal(a.export_data(), b.export_data())
