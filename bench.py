@@ -332,7 +332,9 @@ def run_our_arm(args):
     clocks = clk.summary()
 
     # ---- end to end through the C ABI with host buffers ---------------------
+    # pinned host buffers: psi in, psi out (swapped every step), V
     psi_host = torch.empty(2 * p.n, dtype=torch.float64, pin_memory=True).numpy()
+    psi_next = torch.empty(2 * p.n, dtype=torch.float64, pin_memory=True).numpy()
     V_host = torch.empty(p.n, dtype=torch.float64, pin_memory=True).numpy()
     V_host[:] = V_free
     psi_host[:] = solver.export_data().reshape(-1).view(np.float64)
@@ -347,9 +349,10 @@ def run_our_arm(args):
             solver.load_pote(V_host)
             solver.load_buffer(psi_host)
             solver.real_steps(ITERS_PER_STEP, it)
-            out = solver.export_data()
+            solver.export_async(psi_next)  # widened on the device, copied into pinned memory
+            solver.export_wait()
             e1.record(stream)
-            psi_host[:] = out.reshape(-1).view(np.float64)
+            psi_host, psi_next = psi_next, psi_host
             it += ITERS_PER_STEP
     stream.synchronize()
     barrier(ws)
