@@ -435,9 +435,11 @@ __global__ void __launch_bounds__(256)
     double e[5]        = {0, 0, 0, 0, 0};
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < N;
          q += (size_t)gridDim.x * blockDim.x) {
-        const int k = (int)(q % nz);
-        const int j = (int)((q / nz) % ny);
-        const int i = (int)(q / plane);
+        // grids hold at most 2^30 points: 32-bit index arithmetic
+        const unsigned q32 = (unsigned)q, row = q32 / (unsigned)nz;
+        const int k = (int)(q32 - row * (unsigned)nz);
+        const int i = (int)(row / (unsigned)ny);
+        const int j = (int)(row - (unsigned)i * (unsigned)ny);
         if (i < 1 || i >= nx - 1 || j < 1 || j >= ny - 1 || k < 1 || k >= nz - 1)
             continue;
         auto ld = [&](size_t t) {
