@@ -254,6 +254,22 @@ struct ZArgs {
     int nx, ny;
 };
 
+// Asynchronous global -> shared copies (cp.async, completion per thread; a
+// barrier after the wait makes the data visible to the block).
+__device__ __forceinline__ void cp_async8(void *smem, const void *g) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *g) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most N of this thread's committed groups are pending
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 template <class R, int NZ, int MODE>
 __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
     using C          = cplx<R>;
@@ -274,10 +290,32 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
     C *kb0  = reinterpret_cast<C *>(g_smem); // kinetic tile [k][row]
     C *db0  = kb0 + TK * NZ;                 // dipolar pair tile [m][pair]
     R *phis = reinterpret_cast<R *>(db0 + TD * LD); // phi, then rho, [k][row]
+    R *vs   = phis + TK * NZ;                // V tile [k][row] (real time)
+    C *prs  = db0;                           // kept psi [row][k] (real time, after the C2R)
     __shared__ double red[8];
 
     const C *S_in = reinterpret_cast<const C *>(a.S);
     C *S_out      = reinterpret_cast<C *>(a.S);
+    C *pr         = reinterpret_cast<C *>(a.psi_r);
+    constexpr bool KEPT = MODE == ZM_RT_MID || MODE == ZM_RT_EPI;
+
+    // real time: the kinetic tile and V are copied in (cp.async) behind the C2R
+    if (RT) {
+        const C *pin = reinterpret_cast<const C *>(a.psi_in);
+        const R *Vg  = reinterpret_cast<const R *>(a.V);
+        for (int e = tid; e < RW * NZ; e += NT) {
+            const int row = e / NZ, k = e % NZ;
+            const int rr  = r0 + row;
+            if (rr < rows) {
+                cp_async8(&kb0[row + k * TK], &pin[(size_t)rr * NZ + k]);
+                cp_async4(&vs[row + k * TK], &Vg[(size_t)rr * NZ + k]);
+            } else {
+                kb0[row + k * TK] = C{(R)0, (R)0};
+                vs[row + k * TK]  = (R)0;
+            }
+        }
+        cp_async_commit();
+    }
 
     // ---- phi: dipolar C2R of the row pairs -------------------------------
     if (HAS_INV) {
@@ -319,6 +357,18 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
                 phi_g[(size_t)(r0 + row) * NZ + k] = v;
         }
         __syncthreads();
+        if (KEPT) {
+            // the pair tile is free until the R2C: the kept psi goes there
+            for (int e = tid; e < RW * NZ; e += NT) {
+                const int row = e / NZ, k = e % NZ;
+                const int rr  = r0 + row;
+                if (rr < rows)
+                    cp_async8(&prs[e], &pr[(size_t)rr * NZ + k]);
+                else
+                    prs[e] = C{(R)0, (R)0};
+            }
+            cp_async_commit();
+        }
     } else if (RT) {
         // prologue: phi from the previous calc_fi3d
         const R *phi_g = reinterpret_cast<const R *>(a.phi);
@@ -331,11 +381,10 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
     // ---- psi for the physics step -----------------------------------------
     C *kt = kb0; // tile holding psi in real space, [k][row]
     if (RT) {
-        const C *pin = reinterpret_cast<const C *>(a.psi_in);
-        for (int e = tid; e < RW * NZ; e += NT) {
-            const int row = e / NZ, k = e % NZ;
-            kb0[row + k * TK] = (r0 + row < rows) ? pin[(size_t)(r0 + row) * NZ + k] : C{(R)0, (R)0};
-        }
+        if (KEPT)
+            cp_async_wait<1>(); // kinetic tile and V (the kept psi may still be in flight)
+        else
+            cp_async_wait<0>();
         __syncthreads();
         if (MODE != ZM_RT_PRO)
             ct_fft_ip<+1, R, NZ, RW, TK, NT>(kb0, (const C *)tk.tw, (const C *)tk.lo, tid);
@@ -359,9 +408,11 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
                 gw = (R)c0.gw15;
             }
         }
-        const R *Vg   = reinterpret_cast<const R *>(a.V);
-        C *pr         = reinterpret_cast<C *>(a.psi_r);
         const R hdt   = (R)a.half_dt, cdd = (R)a.cdd, wat = (R)a.w_atoms;
+        if (KEPT) {
+            cp_async_wait<0>();
+            __syncthreads();
+        }
         for (int e = tid; e < RW * NZ; e += NT) {
             const int row = e / NZ, k = e % NZ;
             const int rr  = r0 + row;
@@ -370,11 +421,11 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
             const int i = rr / ny, j = rr - i * ny;
             C p         = kt[row + k * TK];
             if (MODE != ZM_RT_PRO)
-                p = cadd(p, pr[(size_t)rr * NZ + k]); // psi + kinetic increment
+                p = cadd(p, prs[e]); // psi + kinetic increment
             if (i >= 1 && i < nx - 1 && j >= 1 && j < ny - 1 && k >= 1 && k < NZ - 1) {
                 const R dens  = p.x * p.x + p.y * p.y;
                 const R am    = sqrt(dens);
-                const R total = cV * (Vg[(size_t)rr * NZ + k] + cdd * phis[row + k * TK]) + g3 * dens +
+                const R total = cV * (vs[row + k * TK] + cdd * phis[row + k * TK]) + g3 * dens +
                                 gw * (am * am * am);
                 R s, c;
                 sincos_r<R>((R)-0.5 * hdt * total, &s, &c);
@@ -537,7 +588,7 @@ __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {
 
 // Shared memory of k2_z<R, NZ, *>.
 template <class R, int NZ> constexpr size_t z_smem() {
-    return sizeof(cplx<R>) * (33 * NZ + 17 * 2 * NZ) + sizeof(R) * 33 * NZ;
+    return sizeof(cplx<R>) * (33 * NZ + 17 * 2 * NZ) + sizeof(R) * 2 * 33 * NZ;
 }
 
 } // namespace gpe

@@ -231,21 +231,8 @@ struct YZTwid {
     Twid ky, kz, dy, dz;
 };
 
-// Asynchronous global -> shared copies (cp.async, no register staging).
-__device__ __forceinline__ void cp_async8(void *smem, const void *g) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void *smem, const void *g) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// wait until at most N of this thread's committed groups are pending
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-// ROWS x COLS plane (contiguous in global) -> shared rows of stride PS
+// ROWS x COLS plane (contiguous in global) -> shared rows of stride PS, by
+// cp.async (no register staging)
 template <class T, int ROWS, int COLS, int PS, int NT>
 __device__ __forceinline__ void plane_in_async(T *dst, const T *src, int tid) {
     static_assert(sizeof(T) == 8 || sizeof(T) == 4, "8- or 4-byte elements");
