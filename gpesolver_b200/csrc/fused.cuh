@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(NT)
 // -> iFFT_2nx, lower half kept.  scale = 1/(8N) (C2R normalisation) and, in
 // imaginary time, 1/xnorma (the spectrum was built from the unnormalised psi).
 template <class R, int NX, int CNT, int NT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, NX >= 256 ? 2 : 3) // 512-point lines: two CTAs per SM; 256: three
     k3_x_dip(cplx<R> *__restrict__ S, const R *__restrict__ vk, const double *__restrict__ divisor,
              double dip_scale, int ny, int nz, Twid td) {
     using C          = cplx<R>;

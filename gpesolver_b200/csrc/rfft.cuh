@@ -94,6 +94,41 @@ struct LinePass {
         DFTZ<R0, SIGN, R, CMP, IH ? R0 / 2 : R0>::run(a);
     }
 
+    // Stage 0 of every round into the tile: all rounds' global loads are issued
+    // before any butterfly, so a thread keeps ROUNDS0 x R0 loads in flight
+    // (the lines of 512 points take four rounds).
+    template <class Ld> static __device__ __forceinline__ void stage0_to_tile(C *buf, Ld &ld, int tid) {
+        if constexpr (ROUNDS0 == 1) {
+            if (valid<ITEMS0>(tid)) {
+                const int j = tid / COUNT, b = tid - j * COUNT;
+                C a[R0];
+                load0(a, ld, j, b);
+                store0(buf, a, j, b);
+            }
+        } else {
+            C t[ROUNDS0][R0];
+#pragma unroll
+            for (int rd = 0; rd < ROUNDS0; ++rd) {
+                const int it = rd * NT + tid;
+                if (!valid<ITEMS0>(it))
+                    break;
+                const int j = it / COUNT, b = it - j * COUNT;
+#pragma unroll
+                for (int k = 0; k < R0; ++k)
+                    t[rd][k] = (IH && 2 * k >= R0) ? C{(R)0, (R)0} : ld(b, j + k * NR0);
+            }
+#pragma unroll
+            for (int rd = 0; rd < ROUNDS0; ++rd) {
+                const int it = rd * NT + tid;
+                if (!valid<ITEMS0>(it))
+                    break;
+                const int j = it / COUNT, b = it - j * COUNT;
+                DFTZ<R0, SIGN, R, CMP, IH ? R0 / 2 : R0>::run(t[rd]);
+                store0(buf, t[rd], j, b);
+            }
+        }
+    }
+
     static __device__ __forceinline__ void store0(C *buf, const C *a, int j, int b) {
 #pragma unroll
         for (int q = 0; q < R0; ++q)
@@ -143,16 +178,7 @@ struct LinePass {
                 emit(st, a, 0, it);
             }
         } else {
-#pragma unroll
-            for (int rd = 0; rd < ROUNDS0; ++rd) {
-                const int it = rd * NT + tid;
-                if (!valid<ITEMS0>(it))
-                    break;
-                const int j = it / COUNT, b = it - j * COUNT;
-                C a[R0];
-                load0(a, ld, j, b);
-                store0(buf, a, j, b);
-            }
+            stage0_to_tile(buf, ld, tid);
             __syncthreads();
             middle<1>(buf, tw, twlo, tid);
 #pragma unroll
@@ -181,16 +207,7 @@ struct LinePass {
                 load0(a[rd], ld, 0, it);
             }
         } else {
-#pragma unroll
-            for (int rd = 0; rd < ROUNDS0; ++rd) {
-                const int it = rd * NT + tid;
-                if (!valid<ITEMS0>(it))
-                    break;
-                const int j = it / COUNT, b = it - j * COUNT;
-                C t[R0];
-                load0(t, ld, j, b);
-                store0(buf, t, j, b);
-            }
+            stage0_to_tile(buf, ld, tid);
             __syncthreads();
             middle<1>(buf, tw, twlo, tid);
 #pragma unroll
