@@ -415,7 +415,8 @@ def run_our_arm(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64",
-            "data": "synthetic (reference initializers, deterministic)", "config": config_dict(),
+            "data": "synthetic (reference initializers, deterministic)",
+            "config": dict(config_dict(), x_pass_lines_per_cta=list(solver.x_tiles())),
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": int(16 * p.n + 8 * p.n),
                     "d2h_bytes_per_step": int(16 * p.n)},

@@ -111,6 +111,7 @@ SIGNATURES = [
     ("gpe_imag_steps_energies", ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, ctypes.c_int, _dp]),
     ("gpe_real_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_long, ctypes.c_long]),
     ("gpe_launch_count", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    ("gpe_x_tiles", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("gpe_time_kernel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]),
     ("gpe_kernel_name", ctypes.c_char_p, [ctypes.c_int]),
     ("gpe_init_potential", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(gpe_init_params)]),

@@ -56,10 +56,8 @@ enum { ZM_RT_PRO = 0, ZM_RT_MID, ZM_RT_EPI, ZM_IT_PRO, ZM_IT_MID };
 // ---------------------------------------------------------------------------
 // X pencils
 // ---------------------------------------------------------------------------
-// Lines per CTA of the x passes: 16 (an 8-byte complex row segment of 128
-// bytes per line, coalesced); the 512-point dipolar lines then take 64 KB of
-// shared memory per CTA (measured at 256^2 x 64: 70 us against 82 us with 8).
-template <int L> constexpr int xy_count() { return 16; }
+// Lines per CTA of the x passes: 8 or 16 (64 / 128-byte row segments per x),
+// picked per grid by the solver's autotuner (Solver::autotune_x).
 
 // Kinetic x pencils, increment form: psi(x, ky, kz) -> FFT_x ->
 // (exp(i(-dt/2m)k^2) - 1) / N -> iFFT_x, i.e. the change the kinetic step makes
@@ -216,13 +214,6 @@ __global__ void __launch_bounds__(NT) k3_y_dip(cplx<R> *__restrict__ S, int nz, 
 // Shared memory of the x / y passes (one tile of COUNT lines).
 template <class R, int L, int CNT> constexpr size_t xy_smem() { return sizeof(cplx<R>) * CNT * L; }
 
-// Launch shapes of the x pass for nx = N: kinetic (CK lines, NTK threads) and
-// dipolar (CD lines of 2N, NTD threads).
-template <class R, int N> struct XShape {
-    static constexpr int CK = xy_count<N>(), NTK = pass_threads<N, CK>();
-    static constexpr int CD = xy_count<2 * N>(), NTD = pass_threads<2 * N, CD>();
-    static constexpr size_t SK = xy_smem<R, N, CK>(), SD = xy_smem<R, 2 * N, CD>();
-};
 // y pass for ny = N with CNT z columns per tile.
 template <class R, int N, int CNT> struct YShape {
     static constexpr int NTK = pass_threads<N, CNT>(), NTD = pass_threads<2 * N, CNT>();

@@ -16,8 +16,10 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -149,6 +151,7 @@ class SolverBase {
     virtual void it_batch_after(int kind, int count, long long nodes) = 0;
     virtual void it_batch_end()                              = 0;
     virtual const void *psi_ptr() const                      = 0;
+    virtual void x_tiles(int *kin_lines, int *dip_lines) const  = 0;
     virtual int device() const                               = 0;
 };
 
@@ -259,8 +262,10 @@ template <class R> class Solver final : public SolverBase {
         set_divisor_one();
         GPE_CUDA(cudaStreamSynchronize(cur));
         set_smem_attrs();
-        if (fused)
+        if (fused) {
             set_fused_attrs();
+            autotune_x();
+        }
     }
 
     ~Solver() override {
@@ -801,9 +806,8 @@ template <class R> class Solver final : public SolverBase {
             };
 #define GPE_SETX(N)                                                                                \
     if (nx == N) {                                                                                 \
-        using X = XShape<R, N>;                                                                    \
-        set((const void *)k3_x_kin<R, N, X::CK, X::NTK>, X::SK);                                   \
-        set((const void *)k3_x_dip<R, N, X::CD, X::NTD>, X::SD);                                   \
+        set_x_attrs<N, 8>(set);                                                                    \
+        set_x_attrs<N, 16>(set);                                                                   \
     }
 #define GPE_SETY1(N, CNT, SIGN)                                                                    \
     {                                                                                              \
@@ -846,23 +850,109 @@ template <class R> class Solver final : public SolverBase {
 
     // part: 0 both, 1 kinetic only, 2 dipolar only
     // X pass: kinetic pencils (kin, part 0 or 1) and dipolar pencils (part 0, or !kin).
+    // x-pass launches for nx = NN with CNT lines per CTA (the autotuned choice)
+    template <int NN, int CNT, class Set> static void set_x_attrs(Set &set) {
+        set((const void *)k3_x_kin<R, NN, CNT, pass_threads<NN, CNT>()>, xy_smem<R, NN, CNT>());
+        set((const void *)k3_x_dip<R, NN, CNT, pass_threads<2 * NN, CNT>()>, xy_smem<R, 2 * NN, CNT>());
+    }
+    template <int NN, int CNT> void launch_xk(cudaStream_t s) {
+        constexpr int NT = pass_threads<NN, CNT>();
+        launch(k3_x_kin<R, NN, CNT, NT>, (ny * nz + CNT - 1) / CNT, NT, xy_smem<R, NN, CNT>(), s, psi.p,
+               (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, ny, nz, twid(kx));
+    }
+    template <int NN, int CNT> void launch_xd(cudaStream_t s, const double *divisor, double dscale) {
+        constexpr int NT = pass_threads<2 * NN, CNT>();
+        launch(k3_x_dip<R, NN, CNT, NT>, (2 * ny * nz + CNT - 1) / CNT, NT, xy_smem<R, 2 * NN, CNT>(), s, S2.p,
+               (const R *)vk2.p, divisor, dscale, ny, nz, twid(dx));
+    }
+    template <int NN> void f_x_n(cudaStream_t s, bool kin, const double *divisor, int part, double dscale) {
+        if (kin) {
+            if (xk_lines == 8)
+                launch_xk<NN, 8>(s);
+            else
+                launch_xk<NN, 16>(s);
+        }
+        if (!kin || part == 0) {
+            if (xd_lines == 8)
+                launch_xd<NN, 8>(s, divisor, dscale);
+            else
+                launch_xd<NN, 16>(s, divisor, dscale);
+        }
+    }
     void f_x(cudaStream_t s, bool kin, const double *divisor, int part = 0) {
         if constexpr (std::is_same<R, float>::value) {
             const double dscale = 1.0 / (8.0 * (double)N);
 #define GPE_LX(NN)                                                                                 \
-    if (nx == NN) {                                                                                \
-        using X = XShape<R, NN>;                                                                   \
-        if (kin)                                                                                   \
-            launch(k3_x_kin<R, NN, X::CK, X::NTK>, (ny * nz + X::CK - 1) / X::CK, X::NTK, X::SK, s,  \
-                   psi.p, (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, ny, nz,  \
-                   twid(kx));                                                                      \
-        if (!kin || part == 0)                                                                     \
-            launch(k3_x_dip<R, NN, X::CD, X::NTD>, (2 * ny * nz + X::CD - 1) / X::CD, X::NTD, X::SD, \
-                   s, S2.p, (const R *)vk2.p, divisor, dscale, ny, nz, twid(dx));                  \
-    }
+    if (nx == NN)                                                                                  \
+        f_x_n<NN>(s, kin, divisor, part, dscale);
             GPE_XY_CASES(GPE_LX)
 #undef GPE_LX
         }
+    }
+
+    // Autotuner of the x pass: lines per CTA (8 or 16) of the kinetic and of the
+    // dipolar pencils, each timed alone (CUDA events, 5 launches after one
+    // warm-up, on zeroed buffers) when the first solver of a grid is created on a
+    // device; later solvers of that grid and device reuse the choice.
+    // GPE_X_TILES="k,d" (k, d in {8, 16}) fixes the choice instead.
+    void autotune_x() {
+        if (const char *env = std::getenv("GPE_X_TILES")) {
+            int k = 0, d = 0;
+            if (std::sscanf(env, "%d,%d", &k, &d) == 2 && (k == 8 || k == 16) && (d == 8 || d == 16)) {
+                xk_lines = k;
+                xd_lines = d;
+                return;
+            }
+        }
+        static std::mutex mu;
+        static std::map<std::tuple<int, int, int, int>, std::pair<int, int>> chosen;
+        const auto key = std::make_tuple(P.device, nx, ny, nz);
+        std::lock_guard<std::mutex> lock(mu);
+        const auto it = chosen.find(key);
+        if (it != chosen.end()) {
+            xk_lines = it->second.first;
+            xd_lines = it->second.second;
+            return;
+        }
+        GPE_CUDA(cudaMemsetAsync(psi.p, 0, sizeof(C) * N, cur));
+        GPE_CUDA(cudaMemsetAsync(S2.p, 0, sizeof(C) * S2.n, cur));
+        cudaEvent_t e0, e1;
+        GPE_CUDA(cudaEventCreate(&e0));
+        GPE_CUDA(cudaEventCreate(&e1));
+        auto time_of = [&](bool kin) {
+            f_x(cur, kin, nullptr, 1);
+            GPE_CUDA(cudaEventRecord(e0, cur));
+            for (int r = 0; r < 5; ++r)
+                f_x(cur, kin, nullptr, 1);
+            GPE_CUDA(cudaEventRecord(e1, cur));
+            GPE_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            GPE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            return ms;
+        };
+        int best_k = 16, best_d = 16;
+        float tk = 0.f, td = 0.f;
+        for (int c : {16, 8}) {
+            xk_lines = xd_lines = c;
+            const float a = time_of(true), b = time_of(false);
+            if (c == 16 || a < tk) {
+                tk     = a;
+                best_k = c;
+            }
+            if (c == 16 || b < td) {
+                td     = b;
+                best_d = c;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        xk_lines = best_k;
+        xd_lines = best_d;
+        chosen[key] = {best_k, best_d};
+    }
+    void x_tiles(int *k, int *d) const override {
+        *k = xk_lines;
+        *d = xd_lines;
     }
 
     // Y pass (SIGN < 0 forward, > 0 inverse): kinetic lines (kin, part 0 or 1)
@@ -1123,6 +1213,7 @@ template <class R> class Solver final : public SolverBase {
     bool fused = false;
     DevBuf<C> S2;
     DevBuf<C> psir; // real time: psi in real space after the last phase step
+    int xk_lines = 16, xd_lines = 16; // x-pass lines per CTA (autotune_x)
     DevBuf<R> vk2;
     DevBuf<double> zpartial;
     DevBuf<unsigned> ticket;
@@ -1944,6 +2035,14 @@ int gpe_launch_count(gpe_handle *h, long long *count) {
     if (!count)
         return bad("null argument");
     *count = h->impl->launches();
+    return GPE_OK;
+}
+
+int gpe_x_tiles(gpe_handle *h, int *kin_lines, int *dip_lines) {
+    GPE_HANDLE(h);
+    if (!kin_lines || !dip_lines)
+        return bad("null argument");
+    h->impl->x_tiles(kin_lines, dip_lines);
     return GPE_OK;
 }
 

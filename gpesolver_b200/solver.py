@@ -126,6 +126,13 @@ class B200GrossPitaevskiSolver:
         capi.check(self._L.gpe_launch_count(self._h, ctypes.byref(c)))
         return c.value
 
+    def x_tiles(self) -> tuple[int, int]:
+        """Lines per CTA of the kinetic and dipolar x pencils picked by the
+        autotuner for this grid (GPE_X_TILES="k,d" fixes them)."""
+        k, d = ctypes.c_int(), ctypes.c_int()
+        capi.check(self._L.gpe_x_tiles(self._h, ctypes.byref(k), ctypes.byref(d)))
+        return k.value, d.value
+
     # -- data in / out (solver.cpp:118-131, gpu_solver.cpp:136-155) -------
     def load_buffer(self, psi) -> None:
         a = _as_c128_flat(psi, self.n)

@@ -164,6 +164,13 @@ int gpe_imag_steps_energies(gpe_handle *h, long k, int checks, double *e_total);
 /* Number of kernels the library launched on this handle since creation. */
 int gpe_launch_count(gpe_handle *h, long long *count);
 
+/* Lines per CTA of the fused x pass (kinetic, dipolar pencils: 8 or 16) that
+ * the autotuner picked for this grid when the first handle of the grid was
+ * created on its device (GPE_X_TILES="k,d" in the environment fixes them);
+ * 16, 16 on schedules without the fused x pass.  No reference counterpart (the
+ * reference's FFTs are FFTW / cuFFT plans). */
+int gpe_x_tiles(gpe_handle *h, int *kin_lines, int *dip_lines);
+
 /* --- measurement --- */
 
 /* Kernels of the real-time iteration, for per-kernel timing. */
