@@ -890,28 +890,45 @@ template <class R> class Solver final : public SolverBase {
         }
     }
 
-    // Autotuner of the x pass: lines per CTA (8 or 16) of the kinetic and of the
-    // dipolar pencils, each timed alone (CUDA events, 5 launches after one
-    // warm-up, on zeroed buffers) when the first solver of a grid is created on a
-    // device; later solvers of that grid and device reuse the choice.
-    // GPE_X_TILES="k,d" (k, d in {8, 16}) fixes the choice instead.
+    // Autotuner of the pencil passes: lines per CTA (8 or 16) of the kinetic
+    // and of the dipolar x pencils, and (four-kernel schedule, nz >= 16) z
+    // columns per CTA of the y lines, each timed alone (CUDA events, 5 launches
+    // after one warm-up, on zeroed buffers) when the first solver of a grid is
+    // created on a device; later solvers of that grid and device reuse the
+    // choice.  GPE_X_TILES="k,d" and GPE_Y_LINES=c (values 8 or 16) fix them.
     void autotune_x() {
+        y_lines = nz >= 16 ? 16 : 8;
+        bool fix_x = false, fix_y = false;
         if (const char *env = std::getenv("GPE_X_TILES")) {
             int k = 0, d = 0;
             if (std::sscanf(env, "%d,%d", &k, &d) == 2 && (k == 8 || k == 16) && (d == 8 || d == 16)) {
                 xk_lines = k;
                 xd_lines = d;
-                return;
+                fix_x    = true;
             }
         }
+        if (const char *env = std::getenv("GPE_Y_LINES")) {
+            const int c = std::atoi(env);
+            if ((c == 8 || c == 16) && c <= nz) {
+                y_lines = c;
+                fix_y   = true;
+            }
+        }
+        const bool tune_y = !fix_y && !yz_plane() && nz >= 16;
+        if (fix_x && !tune_y)
+            return;
         static std::mutex mu;
-        static std::map<std::tuple<int, int, int, int>, std::pair<int, int>> chosen;
+        static std::map<std::tuple<int, int, int, int>, std::tuple<int, int, int>> chosen;
         const auto key = std::make_tuple(P.device, nx, ny, nz);
         std::lock_guard<std::mutex> lock(mu);
         const auto it = chosen.find(key);
         if (it != chosen.end()) {
-            xk_lines = it->second.first;
-            xd_lines = it->second.second;
+            if (!fix_x) {
+                xk_lines = std::get<0>(it->second);
+                xd_lines = std::get<1>(it->second);
+            }
+            if (tune_y)
+                y_lines = std::get<2>(it->second);
             return;
         }
         GPE_CUDA(cudaMemsetAsync(psi.p, 0, sizeof(C) * N, cur));
@@ -919,36 +936,55 @@ template <class R> class Solver final : public SolverBase {
         cudaEvent_t e0, e1;
         GPE_CUDA(cudaEventCreate(&e0));
         GPE_CUDA(cudaEventCreate(&e1));
-        auto time_of = [&](bool kin) {
-            f_x(cur, kin, nullptr, 1);
+        auto time_of = [&](auto &&run) {
+            run();
             GPE_CUDA(cudaEventRecord(e0, cur));
             for (int r = 0; r < 5; ++r)
-                f_x(cur, kin, nullptr, 1);
+                run();
             GPE_CUDA(cudaEventRecord(e1, cur));
             GPE_CUDA(cudaEventSynchronize(e1));
             float ms = 0.f;
             GPE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
             return ms;
         };
-        int best_k = 16, best_d = 16;
-        float tk = 0.f, td = 0.f;
-        for (int c : {16, 8}) {
-            xk_lines = xd_lines = c;
-            const float a = time_of(true), b = time_of(false);
-            if (c == 16 || a < tk) {
-                tk     = a;
-                best_k = c;
+        int best_k = xk_lines, best_d = xd_lines, best_y = y_lines;
+        if (!fix_x) {
+            float tk = 0.f, td = 0.f;
+            for (int c : {16, 8}) {
+                xk_lines = xd_lines = c;
+                const float a = time_of([&] { f_x(cur, true, nullptr, 1); });
+                const float b = time_of([&] { f_x(cur, false, nullptr, 1); });
+                if (c == 16 || a < tk) {
+                    tk     = a;
+                    best_k = c;
+                }
+                if (c == 16 || b < td) {
+                    td     = b;
+                    best_d = c;
+                }
             }
-            if (c == 16 || b < td) {
-                td     = b;
-                best_d = c;
+        }
+        if (tune_y) {
+            float ty = 0.f;
+            for (int c : {16, 8}) {
+                y_lines       = c;
+                const float a = time_of([&] {
+                    f_y<+1>(cur, true);
+                    f_y<-1>(cur, true);
+                });
+                if (c == 16 || a < ty) {
+                    ty     = a;
+                    best_y = c;
+                }
             }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         xk_lines = best_k;
         xd_lines = best_d;
-        chosen[key] = {best_k, best_d};
+        y_lines  = best_y;
+        if (!fix_x && !fix_y) // only measured choices are shared
+            chosen[key] = std::make_tuple(best_k, best_d, best_y);
     }
     void x_tiles(int *k, int *d) const override {
         *k = xk_lines;
@@ -959,7 +995,7 @@ template <class R> class Solver final : public SolverBase {
     // and dipolar lines (part 0, or !kin).  Tiles of 16 z columns (8 when nz = 8).
     template <int SIGN> void f_y(cudaStream_t s, bool kin, int part = 0) {
         if constexpr (std::is_same<R, float>::value) {
-            if (nz >= 16)
+            if (y_lines == 16)
                 f_y_cnt<SIGN, 16>(s, kin, part);
             else
                 f_y_cnt<SIGN, 8>(s, kin, part);
@@ -1214,6 +1250,7 @@ template <class R> class Solver final : public SolverBase {
     DevBuf<C> S2;
     DevBuf<C> psir; // real time: psi in real space after the last phase step
     int xk_lines = 16, xd_lines = 16; // x-pass lines per CTA (autotune_x)
+    int y_lines = 16;                 // y-pass z columns per CTA (four-kernel schedule; autotune_x)
     DevBuf<R> vk2;
     DevBuf<double> zpartial;
     DevBuf<unsigned> ticket;

@@ -1,5 +1,6 @@
-"""The x-pass autotuner (GPU): the tile widths it chooses between give the same
-bits, and a grid's choice is made once per device and reused."""
+"""The pencil-pass autotuner (GPU): the tile widths it chooses between (x
+pencils, y lines) give the same bits, and a grid's choice is made once per
+device and reused."""
 import numpy as np
 import pytest
 
@@ -39,3 +40,19 @@ def test_autotuner_choice_is_reused_per_grid(monkeypatch):
         assert b.x_tiles() == a.x_tiles()
     with G.B200GrossPitaevskiSolver(p, precision="c128") as c:
         assert c.x_tiles() == (16, 16)  # no fused x pass in FP64
+
+
+def test_y_column_choices_give_identical_results(monkeypatch):
+    # four-kernel schedule: z columns per CTA of the y lines
+    p = gparams(WELL_CONDITIONED(32, 256, 16))
+    V, psi0 = G.potential(p), G.initial_psi(p)
+    outs = []
+    for cols in ("16", "8"):
+        monkeypatch.setenv("GPE_Y_LINES", cols)
+        with G.B200GrossPitaevskiSolver(p) as s:
+            s.load_pote(V)
+            s.load_buffer(psi0)
+            s.imag_steps(20)
+            s.real_steps(20, 0)
+            outs.append(s.export_data())
+    np.testing.assert_array_equal(outs[1], outs[0])
