@@ -393,6 +393,11 @@ template <class R> class Solver final : public SolverBase {
     void it_batch_begin() override {
         if (!lazy)
             set_divisor_one();
+        // members of a batch run side by side: fewer, larger CTAs of the dipolar
+        // x pencils pay there (64-member sweep: 76.8 k against 75.7 k
+        // member-iterations/s with the widths tuned for a solve alone)
+        if (std::getenv("GPE_X_TILES") == nullptr)
+            xd_lines = 16;
     }
     // Records this solver's fused IT graph piece (kind 20: prologue, 21: `count`
     // iterations) on its capture stream as a branch from `fork` that joins `root`.
