@@ -441,11 +441,15 @@ def run_our_arm(args):
         dist.destroy_process_group()
 
 
-def run_profile(iters: int) -> None:
-    """A short run of the RT kernels for a profiler's launch list (no timing)."""
+def run_profile(iters: int, grid: str = "") -> None:
+    """A short run of the RT kernels for a profiler's launch list (no timing);
+    grid "nx,ny,nz" replaces the workload's 128x128x32."""
     import gpesolver_b200 as G
 
-    p = G.params_from_json(workload_json())
+    j = workload_json()
+    if grid:
+        j["nx"], j["ny"], j["nz"] = (int(v) for v in grid.split(","))
+    p = G.params_from_json(j)
     with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
         s.load_pote(G.potential(p))
         s.load_buffer(G.initial_psi(p))
@@ -922,9 +926,10 @@ def main():
     ap.add_argument("--profile", type=int, default=0,
                     help="profiling run: set up the workload (10 IT iterations), then run this many "
                          "RT iterations untimed and exit")
+    ap.add_argument("--profile-grid", default="", help="nx,ny,nz of the profiling run (default 128,128,32)")
     args = ap.parse_args()
     if args.profile:
-        run_profile(args.profile)
+        run_profile(args.profile, args.profile_grid)
         return
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
