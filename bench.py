@@ -182,8 +182,21 @@ def reference_cpu_rate(budget_s: float, min_iters: int = 3, max_iters: int = 200
     dt = time.perf_counter() - t0
     S.close()
     return {"value": n / dt, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{n} RT iterations at {NX}x{NY}x{NZ} after 2 IT iterations, "
-                      f"fftw_n_threads={threads} (FP64 FFTW-API shim; FFTW3 absent on this image)"}
+            "sample": f"{n} RT iterations at {NX}x{NY}x{NZ} after 2 IT iterations (a bounded sample: the "
+                      f"rate does not depend on the state), fftw_n_threads={threads} (FP64 FFTW-API shim; "
+                      f"FFTW3 absent on this image)"}
+
+
+def fft_check(threads: int) -> dict:
+    """How fast the CPU baseline's FFT is: the FP64 FFTW-API shim (FFTW3 is not in
+    this image) beside numpy / scipy pocketfft on the reference's padded dipolar
+    r2c + c2r pair (256x256x64 for this grid), same host."""
+    from oracle import oracle as O
+
+    out = O.fft_backend_check((2 * NX, 2 * NY, 2 * NZ), threads)
+    out["note"] = ("the CPU baseline's FFTs run on the shim; a production FFT (FFTW3, absent here) "
+                   "would make the reference's CPU iterations faster than reported")
+    return out
 
 
 def reference_gpu_rate(iters: int = 200) -> dict | None:
@@ -221,7 +234,9 @@ def run_reference_arm(args):
                            pote_strategy="MEXICAN", fftw_n_threads=threads)
     kind = "reference" if O.ref_available() else "port"
     S = O.RefSolver(cfg) if kind == "reference" else O.OracleSolver(cfg)
-    S.imag_steps(2)
+    t_setup = time.perf_counter()
+    S.imag_steps(args.ref_it_setup)  # untimed set-up: the workload's imaginary-time phase
+    t_setup = time.perf_counter() - t_setup
     S.change_potential("MEXICAN_FREE")
     per_step = args.ref_iters_per_step
     it = 0
@@ -235,14 +250,17 @@ def run_reference_arm(args):
     dt = time.perf_counter() - t0
     S.close()
     value = args.steps * per_step / dt
-    sample = (f"{per_step} RT iterations per step at {NX}x{NY}x{NZ}, fftw_n_threads={threads} "
+    sample = (f"{per_step} RT iterations per step at {NX}x{NY}x{NZ} (a bounded sample of the 1000 per step "
+              f"of this arm's config), after {args.ref_it_setup} untimed IT iterations "
+              f"({t_setup:.0f} s) and the switch to MEXICAN_FREE; fftw_n_threads={threads} "
               f"(FP64 FFTW-API shim; FFTW3 absent on this image)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (reference initializers, deterministic)", "config": config_dict(),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample,
+                         "fft_backend_check": fft_check(threads)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -277,6 +295,58 @@ def measured_peak():
             return float(json.load(f)["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
+
+
+LONG_RT_FIXTURE = os.path.join(ROOT, "tests", "golden", "readme_fs_long_rt.npz")
+
+
+def accuracy_vs_reference_fixture(path: str = LONG_RT_FIXTURE) -> dict | None:
+    """The complex64 path on the README full simulation (1000 IT iterations,
+    MEXICAN_FREE, 10000 RT iterations) against the reference's own FP64 run of
+    the same simulation (tests/golden/readme_fs_long_rt.npz, written by
+    tests/golden/gen_long_rt.py from the compiled reference): psi relative L2,
+    energy relative error and norm drift at each saved checkpoint."""
+    import numpy as np
+
+    import gpesolver_b200 as G
+
+    if not os.path.exists(path):
+        return None
+    fx = np.load(path)
+    steps = [int(v) for v in fx["meta_steps"]]
+    n_it, checkpoints = steps[0], steps[1:]
+    p = G.params_from_json(workload_json())
+    rows = []
+    with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
+        s.init_pote()
+        s.init_buffer()
+        s.imag_steps(n_it)
+
+        def compare(psi_ref, e_ref, norm_ref, norm0_ref, norm0):
+            psi = s.export_data().reshape(-1)
+            want = psi_ref.astype(np.complex128).reshape(-1)
+            e = s.calc_energy().e_total
+            return {"psi_rel_l2": float(np.linalg.norm(psi - want) / np.linalg.norm(want)),
+                    "energy_rel": float(abs(e - e_ref[5]) / abs(e_ref[5])),
+                    "norm_drift": float(s.calc_norm() / norm0 - 1.0),
+                    "reference_norm_drift": float(norm_ref / norm0_ref - 1.0)}
+
+        norm0, norm0_ref = s.calc_norm(), float(fx["norm_it"][0])
+        row = compare(fx["psi_it"], fx["energy_it"], norm0_ref, norm0_ref, norm0)
+        rows.append(dict(phase="IT", iterations=n_it, **row))
+        s.init_pote("MEXICAN_FREE")
+        norm0 = s.calc_norm()
+        done = 0
+        for k in checkpoints:
+            s.real_steps(k - done, done)
+            done = k
+            row = compare(fx[f"psi_rt_{k}"], fx[f"energy_rt_{k}"], float(fx[f"norm_rt_{k}"][0]), norm0_ref,
+                          norm0)
+            rows.append(dict(phase="RT", iterations=k, **row))
+    return {"workload": "README full simulation at 128x128x32: 1000 IT, MEXICAN_FREE, 10000 RT",
+            "reference": "the reference's CpuGrossPitaevskiSolver compiled from its sources, FP64 "
+                         "(FP64 FFTW-API shim), psi stored as complex64",
+            "target": "psi relative L2 <= 1e-5 after 10000 RT iterations", "checkpoints": rows}
 
 
 def run_our_arm(args):
@@ -391,9 +461,12 @@ def run_our_arm(args):
     F = 8.0 * p.n
     R4 = 4.0 * p.n
     I = 8.0 * NX * 2 * NY * (NZ + 1)
-    # algorithmic bytes per RT iteration (fused schedule; 2F of them the
-    # real-space psi that the increment form keeps between phase steps)
-    b_rt = 8 * F + 3 * R4 + 4 * I
+    # algorithmic bytes per RT iteration of the minimal fused schedule:
+    # B_RT = 6F + 3R + 4I.  The increment form of the kinetic step also reads and
+    # writes the real-space psi it keeps between phase steps (2F more): that
+    # implementation figure is reported beside it, not in the fraction.
+    b_rt = 6 * F + 3 * R4 + 4 * I
+    b_impl = 8 * F + 3 * R4 + 4 * I
     per_gpu_rate = args.steps * ITERS_PER_STEP / (t_ms / 1e3)
     traffic = traffic_from_profiles(kname)
 
@@ -403,12 +476,25 @@ def run_our_arm(args):
     if rank == 0 and ws == 1 and not args.no_ref_gpu:
         ref_gpu = reference_gpu_rate()
 
+    # imaginary time at the plain IT run's grid and at this grid, and the
+    # complex64 path against the reference's FP64 run after 10k RT iterations
+    imag, accuracy = None, None
+    if rank == 0 and ws == 1 and not args.no_extras:
+        imag = []
+        for desc, over in IMAG_CASES:
+            m = measure_imag(dict(workload_json("IT"), **over), steps=5, warmup=3)
+            imag.append({"workload": desc, "grid": m["grid"], "value": m["value"], "unit": m["unit"],
+                         "steps": m["steps"], "iterations_per_step": m["iterations_per_step"],
+                         "roofline_step": m["roofline_step"], "clocks": m["clocks"]})
+        accuracy = accuracy_vs_reference_fixture()
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = reference_cpu_rate(args.cpu_budget)
         # the reference's default fftw_n_threads (parameters.cpp:30) beside it
         four = reference_cpu_rate(args.cpu_budget / 2, threads=4)
         cpu["fftw_n_threads_4"] = {"value": four["value"], "sample": four["sample"]}
+        cpu["fft_backend_check"] = fft_check(cpu["cores"])
 
     if rank == 0:
         line = {
@@ -426,12 +512,17 @@ def run_our_arm(args):
                          "traffic": traffic, "algorithmic_bytes_per_launch": by,
                          "launch_ms": ms},
             "roofline_step": {"algorithmic_bytes_per_iteration": b_rt,
-                              "achieved": b_rt * per_gpu_rate / 1e9, "peak": peak, "unit": "GB/s",
-                              "frac": b_rt * per_gpu_rate / 1e9 / peak},
+                              "definition": "B_RT = 6F + 3R + 4I, F = 8N, R = 4N, I = 8 nx 2ny (nz+1)",
+                              "achieved": b_rt * per_gpu_rate / 1e9, "peak": peak, "peak_kind": peak_kind,
+                              "unit": "GB/s", "frac": b_rt * per_gpu_rate / 1e9 / peak,
+                              "implementation_bytes_per_iteration": b_impl,
+                              "implementation_frac": b_impl * per_gpu_rate / 1e9 / peak},
             "kernels_ms": {k: round(v[0], 5) for k, v in kt.items()},
             "clocks": clocks,
             "cpu_baseline": cpu,
             "reference_gpu": ref_gpu,
+            "imag": imag,
+            "accuracy_vs_fp64_reference": accuracy,
         }
         print(json.dumps(line), flush=True)
     solver.close()
@@ -485,72 +576,94 @@ def reference_it_seconds(grid, budget_s: float) -> tuple[float, int]:
     return dt / n, n
 
 
+IMAG_CASES = [
+    ("plain imaginary-time run, 64x64x16, HARMONIC (60, 60, 120) Hz, GAUSS, edd=1.5, n_atoms=2e4",
+     dict(nx=64, ny=64, nz=16, pote_strategy="HARMONIC", init_strategy="GAUSS")),
+    ("imaginary-time phase of the README run, 128x128x32, MEXICAN(dd=1500 nm), MULTIPLE_GAUSS(2)", {}),
+]
+
+
+def b_it_bytes(nx: int, ny: int, nz: int) -> float:
+    """Algorithmic bytes of one imaginary-time iteration: B_IT = 2F + 3R + 4I
+    (F = 8N complex64 psi, R = 4N FP32 field, I = 8 nx 2ny (nz+1) pruned
+    dipolar intermediate)."""
+    n = nx * ny * nz
+    return 2 * 8.0 * n + 3 * 4.0 * n + 4 * 8.0 * nx * 2 * ny * (nz + 1)
+
+
+def measure_imag(j: dict, steps: int, warmup: int, iters: int = ITERS_PER_STEP) -> dict:
+    """Imaginary-time iterations/s of one configuration: `steps` timed steps of
+    `iters` iterations (CUDA events on the solver's stream, L2 flushed between
+    steps), after `warmup` untimed steps."""
+    import torch
+
+    import gpesolver_b200 as G
+
+    p = G.params_from_json(j)
+    s = G.B200GrossPitaevskiSolver(p, precision="c64")
+    stream = torch.cuda.Stream()
+    s.set_stream(stream.cuda_stream)
+    s.init_pote()
+    s.init_buffer()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            s.imag_steps(iters)
+    stream.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    l0 = s.launch_count()
+    with ClockSampler(0) as clk:
+        with torch.cuda.stream(stream):
+            for e0, e1 in evs:
+                flush.zero_()
+                e0.record(stream)
+                s.imag_steps(iters)
+                e1.record(stream)
+        stream.synchronize()
+    launches = s.launch_count() - l0
+    t_ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+    e = s.calc_energy().e_total
+    s.close()
+    peak, peak_kind = measured_peak()
+    value = steps * iters / (t_ms / 1e3)
+    b_it = b_it_bytes(p.nx, p.ny, p.nz)
+    return {"grid": [p.nx, p.ny, p.nz], "value": value, "unit": "iterations/s", "t_ms": t_ms,
+            "steps": steps, "iterations_per_step": iters, "gpu_launches": launches,
+            "energy_after": e, "clocks": clk.summary(),
+            "roofline_step": {"algorithmic_bytes_per_iteration": b_it, "achieved": b_it * value / 1e9,
+                              "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                              "frac": b_it * value / 1e9 / peak}}
+
+
 def run_imag(args):
     """Imaginary-time iterations/s (the reference's imag_time_iter: dipolar phi,
     Euler update, norm, normalisation) for the plain imaginary-time run (64^2 x
     16, HARMONIC, GAUSS) and at 128^2 x 32 (the README run's IT phase), one JSON
     line per grid, with the whole iteration against B_IT = 2F + 3R + 4I and the
     reference's CPU code timed beside it."""
-    import numpy as np
     import torch
 
-    import gpesolver_b200 as G
-
     torch.cuda.set_device(0)
-    peak, peak_kind = measured_peak()
-    cases = [("plain imaginary-time run, 64x64x16, HARMONIC (60, 60, 120) Hz, GAUSS, edd=1.5, n_atoms=2e4",
-              dict(workload_json("IT"), nx=64, ny=64, nz=16, pote_strategy="HARMONIC", init_strategy="GAUSS")),
-             ("imaginary-time phase of the README run, 128x128x32, MEXICAN(dd=1500 nm), MULTIPLE_GAUSS(2)",
-              workload_json("IT"))]
-    for desc, j in cases:
-        p = G.params_from_json(j)
-        s = G.B200GrossPitaevskiSolver(p, precision="c64")
-        stream = torch.cuda.Stream()
-        s.set_stream(stream.cuda_stream)
-        s.init_pote()
-        s.init_buffer()
-        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
-        with torch.cuda.stream(stream):
-            for _ in range(args.warmup):
-                s.imag_steps(ITERS_PER_STEP)
-        stream.synchronize()
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(args.steps)]
-        l0 = s.launch_count()
-        with ClockSampler(0) as clk:
-            with torch.cuda.stream(stream):
-                for e0, e1 in evs:
-                    flush.zero_()
-                    e0.record(stream)
-                    s.imag_steps(ITERS_PER_STEP)
-                    e1.record(stream)
-            stream.synchronize()
-        launches = s.launch_count() - l0
-        t_ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-        value = args.steps * ITERS_PER_STEP / (t_ms / 1e3)
-        e = s.calc_energy().e_total
-        s.close()
-        F, R4 = 8.0 * p.nx * p.ny * p.nz, 4.0 * p.nx * p.ny * p.nz
-        I = 8.0 * p.nx * 2 * p.ny * (p.nz + 1)
-        b_it = 2 * F + 3 * R4 + 4 * I
+    for desc, over in IMAG_CASES:
+        j = dict(workload_json("IT"), **over)
+        m = measure_imag(j, args.steps, args.warmup)
         cpu = None
         if not args.no_cpu_baseline:
             sec, n = reference_it_seconds_cfg(j, args.cpu_budget)
             cpu = {"value": 1.0 / sec, "unit": "iterations/s", "cores": os.cpu_count() or 1,
-                   "kind": "reference", "sample": f"{n} IT iterations at {p.nx}x{p.ny}x{p.nz}, "
+                   "kind": "reference", "sample": f"{n} IT iterations at {j['nx']}x{j['ny']}x{j['nz']}, "
                    f"fftw_n_threads={os.cpu_count() or 1} (FP64 FFTW-API shim; FFTW3 absent on this image)"}
+        nx, ny, nz = m["grid"]
         print(json.dumps({
-            "metric": f"imaginary-time iterations/s at {p.nx}x{p.ny}x{p.nz}", "value": value,
+            "metric": f"imaginary-time iterations/s at {nx}x{ny}x{nz}", "value": m["value"],
             "unit": "iterations/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": m["t_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64", "data": "synthetic (reference initializers, deterministic)",
-            "config": {"workload": desc, "grid": [p.nx, p.ny, p.nz], "iterations_per_step": ITERS_PER_STEP,
+            "config": {"workload": desc, "grid": m["grid"], "iterations_per_step": ITERS_PER_STEP,
                        "l2": "flushed between timed steps (256 MiB write)"},
-            "gpu_launches": launches,
-            "roofline_step": {"algorithmic_bytes_per_iteration": b_it, "achieved": b_it * value / 1e9,
-                              "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                              "frac": b_it * value / 1e9 / peak},
-            "energy_after": e, "clocks": clk.summary(), "cpu_baseline": cpu}), flush=True)
+            "gpu_launches": m["gpu_launches"], "roofline_step": m["roofline_step"],
+            "energy_after": m["energy_after"], "clocks": m["clocks"], "cpu_baseline": cpu}), flush=True)
 
 
 def reference_it_seconds_cfg(j: dict, budget_s: float) -> tuple[float, int]:
@@ -909,8 +1022,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-iters-per-step", type=int, default=2)
+    ap.add_argument("--ref-it-setup", type=int, default=1000,
+                    help="imaginary-time iterations the reference arm runs (untimed) before its RT steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's GPU backend")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the imaginary-time rates and the accuracy check of the default line")
     ap.add_argument("--workload", default="rt", choices=["rt", "imag", "sweep", "accuracy", "warmstart"],
                     help="rt: the headline real-time benchmark; imag: imaginary-time iterations/s; "
                          "sweep: 64 batched imaginary-time solves")

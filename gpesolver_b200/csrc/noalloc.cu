@@ -14,14 +14,16 @@
 //    the V_dd(k) table ((nx+1) * (ny+1) * (nz+1) floats) and three twiddle
 //    tables with their rounding remainders; grids needing more than GPE_NOALLOC_SCRATCH_BYTES are rejected
 //    with GPE_ERR_SIZE (128 x 128 x 32 needs about 10.9 MB);
-//  * the array lives on every GPU that loads the library until the process
+//   * the array lives on every GPU that loads the library until the process
 //    exits, and every call on a GPU shares it: calls that overlap on that GPU
-//    (other streams, other threads) race, and each call rebuilds the tables
-//    it needs unless the previous call on that GPU used the same grid;
+//    (other streams, other threads) race.  Every call rebuilds the twiddle and
+//    V_dd(k) tables it needs before its passes (a few microseconds): no state
+//    carries over from one call to the next, whatever stream or grid the
+//    previous call used;
 //  * the first call on each device does a one-time set-up on the host (looks
 //    up the array's device address with cudaGetSymbolAddress and raises the
-//    kernels' shared-memory limit); make that first call before any stream
-//    capture on that device.
+//    kernels' shared-memory limit to the device's opt-in maximum); make that
+//    first call before any stream capture on that device.
 #include "../../include/gpe_b200.h"
 #include "kernels.cuh"
 #include "plan.hpp"
@@ -40,11 +42,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[GPE_NOALLOC_SCR
 constexpr int kMaxDevices = 64;
 
 struct NoallocSlot {
-    bool ready           = false;
-    unsigned char *base  = nullptr; // device address of g_noalloc_scratch
-    // grid of the tables currently in the scratch
-    int nx = 0, ny = 0, nz = 0;
-    double dx = 0, dy = 0, dz = 0;
+    bool ready          = false;
+    unsigned char *base = nullptr; // device address of g_noalloc_scratch
+    size_t smem_max     = 0;       // dynamic shared memory the kernels may use on this device
 };
 
 std::mutex g_noalloc_mu;
@@ -164,7 +164,6 @@ extern "C" int gpe_calc_fi3d_noalloc(const void *psi_c64_dev, float *fi3d_dev, i
     const size_t smz = 2 * sizeof(float2) * (size_t)(TBz + 1) * lz.L; // z tiles: odd stride TB + 1
 
     NoallocSlot &slot = g_noalloc_slots[dev];
-    bool rebuild      = false;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
         if (!slot.ready) {
@@ -174,28 +173,32 @@ extern "C" int gpe_calc_fi3d_noalloc(const void *psi_c64_dev, float *fi3d_dev, i
             err     = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (err != cudaSuccess)
                 return fail(GPE_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(err));
+            int optin = 0;
+            err       = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+            if (err != cudaSuccess)
+                return fail(GPE_ERR_CUDA, std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(err));
             const void *kern[] = {(const void *)k_dip_z_fwd<float>, (const void *)k_dip_y<-1, float>,
                                   (const void *)k_dip_y<+1, float>, (const void *)k_dip_x<float>,
                                   (const void *)k_dip_z_inv<float>};
             for (const void *f : kern) {
-                err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+                err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
                 if (err != cudaSuccess)
                     return fail(GPE_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(err));
             }
-            slot.base  = static_cast<unsigned char *>(p);
-            slot.ready = true;
-        }
-        if (slot.nx != nx || slot.ny != ny || slot.nz != nz || slot.dx != dx || slot.dy != dy ||
-            slot.dz != dz) {
-            rebuild  = true;
-            slot.nx  = nx;
-            slot.ny  = ny;
-            slot.nz  = nz;
-            slot.dx  = dx;
-            slot.dy  = dy;
-            slot.dz  = dz;
+            slot.base     = static_cast<unsigned char *>(p);
+            slot.smem_max = (size_t)optin;
+            slot.ready    = true;
         }
     }
+    if (smx > slot.smem_max || smy > slot.smem_max || smz > slot.smem_max)
+        return fail(GPE_ERR_SIZE, "gpe_calc_fi3d_noalloc: the line tiles of this grid need more shared memory "
+                                  "than the device allows per block");
+    // An error left by earlier, unrelated work would be reported as this call's:
+    // refuse to start instead (the error stays pending for its owner).
+    err = cudaPeekAtLastError();
+    if (err != cudaSuccess)
+        return fail(GPE_ERR_CUDA, std::string("gpe_calc_fi3d_noalloc: a CUDA error from earlier work is pending: ") +
+                                      cudaGetErrorString(err));
     unsigned char *base = slot.base;
     float2 *A           = reinterpret_cast<float2 *>(base + lay.a_off);
     float *vk           = reinterpret_cast<float *>(base + lay.vk_off);
@@ -210,12 +213,12 @@ extern "C" int gpe_calc_fi3d_noalloc(const void *psi_c64_dev, float *fi3d_dev, i
     lz.twlo             = twz + 2 * nz;
     const int H         = nz + 1;
 
-    if (rebuild) {
-        k_na_twiddles<<<(2 * nx + 255) / 256, 256, 0, s>>>(twx, twx + 2 * nx, 2 * nx);
-        k_na_twiddles<<<(2 * ny + 255) / 256, 256, 0, s>>>(twy, twy + 2 * ny, 2 * ny);
-        k_na_twiddles<<<(2 * nz + 255) / 256, 256, 0, s>>>(twz, twz + 2 * nz, 2 * nz);
-        k_na_vdip<<<592, 256, 0, s>>>(vk, nx, ny, nz, dx, dy, dz);
-    }
+    // the tables of this grid, rebuilt by every call (in stream order before the
+    // passes that read them)
+    k_na_twiddles<<<(2 * nx + 255) / 256, 256, 0, s>>>(twx, twx + 2 * nx, 2 * nx);
+    k_na_twiddles<<<(2 * ny + 255) / 256, 256, 0, s>>>(twy, twy + 2 * ny, 2 * ny);
+    k_na_twiddles<<<(2 * nz + 255) / 256, 256, 0, s>>>(twz, twz + 2 * nz, 2 * nz);
+    k_na_vdip<<<592, 256, 0, s>>>(vk, nx, ny, nz, dx, dy, dz);
     // The pruned dipolar convolution: every element of A that a pass reads was
     // written by the pass before it in this call, so nothing needs clearing.
     const int lines = nx * ny;

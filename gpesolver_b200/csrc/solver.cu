@@ -924,8 +924,10 @@ template <class R> class Solver final : public SolverBase {
         if (fix_x && !tune_y)
             return;
         static std::mutex mu;
-        static std::map<std::tuple<int, int, int, int>, std::tuple<int, int, int>> chosen;
-        const auto key = std::make_tuple(P.device, nx, ny, nz);
+        // keyed by the schedule too: the plane schedule never tunes y_lines, so a
+        // four-kernel solver of the same grid must not reuse its untuned value
+        static std::map<std::tuple<int, int, int, int, bool>, std::tuple<int, int, int>> chosen;
+        const auto key = std::make_tuple(P.device, nx, ny, nz, yz_plane());
         std::lock_guard<std::mutex> lock(mu);
         const auto it = chosen.find(key);
         if (it != chosen.end()) {

@@ -313,7 +313,8 @@ int gpe_load_amplitude_device(gpe_handle *h, const float *amp_dev, size_t n);
  *   cuda_stream  cudaStream_t to launch on (NULL: the legacy default stream)
  * Grids whose scratch exceeds the limit are rejected with GPE_ERR_SIZE
  * (128 x 128 x 32 needs about 10.9 MB).  All calls on a GPU share the array, so
- * calls that overlap on one GPU race.  The first call on each device does a
+ * calls that overlap on one GPU race; each call rebuilds the tables it needs,
+ * so nothing carries over from one call to the next.  The first call on each device does a
  * one-time host-side set-up (device address of the array, kernel attributes);
  * make it before any stream capture on that device. */
 int gpe_calc_fi3d_noalloc(const void *psi_c64_dev, float *fi3d_dev, int nx, int ny, int nz,

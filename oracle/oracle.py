@@ -584,3 +584,68 @@ class RefGpuSolver:
         rglib().gperefgpu_energy(_ptr(out))
         return out
 
+
+
+# ---------------------------------------------------------------------------
+# Speed of the FP64 FFTW-API shim beside numpy / scipy pocketfft
+# ---------------------------------------------------------------------------
+def shim_fft_seconds(shape=(256, 256, 64), threads: int = 1, reps: int = 3) -> float:
+    """Seconds for one r2c + c2r pair of `shape` through the FP64 FFTW-API shim
+    (the padded dipolar transform pair the reference runs every calc_fi3d,
+    src/solver/fft_solvers/cpu/fftw_poisson_solver.cpp:51-96), best of `reps`."""
+    import time
+
+    L = ctypes.CDLL(ORACLE_SO)
+    L.fftw_plan_dft_r2c_3d.restype = ctypes.c_void_p
+    L.fftw_plan_dft_r2c_3d.argtypes = [ctypes.c_int] * 3 + [_dp, _dp, ctypes.c_uint]
+    L.fftw_plan_dft_c2r_3d.restype = ctypes.c_void_p
+    L.fftw_plan_dft_c2r_3d.argtypes = [ctypes.c_int] * 3 + [_dp, _dp, ctypes.c_uint]
+    L.fftw_execute.argtypes = [ctypes.c_void_p]
+    L.fftw_destroy_plan.argtypes = [ctypes.c_void_p]
+    L.fftw_plan_with_nthreads.argtypes = [ctypes.c_int]
+    L.fftw_plan_with_nthreads(threads)
+    n0, n1, n2 = shape
+    x = np.random.default_rng(0).standard_normal(n0 * n1 * n2)
+    spec = np.zeros(2 * n0 * n1 * (n2 // 2 + 1))
+    back = np.zeros_like(x)
+    fwd = L.fftw_plan_dft_r2c_3d(n0, n1, n2, _ptr(x), _ptr(spec), 0)
+    inv = L.fftw_plan_dft_c2r_3d(n0, n1, n2, _ptr(spec), _ptr(back), 0)
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        L.fftw_execute(fwd)
+        L.fftw_execute(inv)
+        best = min(best, time.perf_counter() - t0)
+    L.fftw_destroy_plan(fwd)
+    L.fftw_destroy_plan(inv)
+    return best
+
+
+def fft_backend_check(shape=(256, 256, 64), threads: int = 1, reps: int = 3) -> dict:
+    """The shim's r2c + c2r time for `shape` beside numpy's pocketfft (one
+    thread) and scipy's pocketfft with `threads` workers, FP64, same host: how
+    the CPU baseline's FFT compares with a production FFT library."""
+    import time
+
+    x = np.random.default_rng(0).standard_normal(shape)
+
+    def best(fn):
+        t = float("inf")
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            t = min(t, time.perf_counter() - t0)
+        return t
+
+    out = {"shape": list(shape), "threads": threads,
+           "shim_r2c_c2r_s": shim_fft_seconds(shape, threads, reps),
+           "shim_r2c_c2r_s_1_thread": shim_fft_seconds(shape, 1, reps),
+           "numpy_pocketfft_r2c_c2r_s_1_thread": best(lambda: np.fft.irfftn(np.fft.rfftn(x), s=shape))}
+    try:
+        import scipy.fft as sf
+
+        out["scipy_pocketfft_r2c_c2r_s"] = best(lambda: sf.irfftn(sf.rfftn(x, workers=threads), s=shape,
+                                                                  workers=threads))
+    except ImportError:
+        pass
+    return out

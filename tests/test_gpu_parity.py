@@ -48,32 +48,20 @@ def test_single_operations_match_golden(name, prec):
         np.testing.assert_allclose(e, g["op_energy"], rtol=ETOL[prec], atol=1e-30 + ETOL[prec] * abs(g["op_energy"][5]))
 
 
-def _rt_phase_max(name, g):
-    """Largest nonlinear + external phase of one RT half step at the start of the
-    RT phase of a fixture, from the FP64 golden data."""
-    over, n_it, switch, n_rt, first = golden_cases().CASES[name]
-    p = O.make_params(O.default_config(**over))
-    psi = c128(g["it_psi"] if n_it else g["psi0"])
-    V = g["pote1"] if switch else g["pote0"]
-    fi = g["it_fi3d"] if n_it else np.zeros_like(V)
-    d = np.abs(psi) ** 2
-    th = 0.5 * p.real_time_dt * (V + p.cdd * fi + (p.ggp11 - p.cdd / 3) * d * p.n_atoms
-                                 + p.gamma * np.abs(psi) ** 3 * p.w_15)
-    return float(np.abs(th).max())
-
-
 @pytest.mark.parametrize("prec", ["c128", "c64"])
 @pytest.mark.parametrize("name", CASES)
 def test_fused_iterations_match_golden(name, prec):
+    """IT then RT iterations against the compiled reference's fixtures.  In
+    complex64 the real-time phase is compared on the well-conditioned fixtures
+    only (WELL_CONDITIONED in gen_golden.py): on the others the imaginary-time
+    state is a collapsing droplet whose nonlinear phase reaches 5-80 rad per
+    half step, so the FP64 reference itself magnifies a change of its start at
+    the 1e-7 level (complex64 rounding) far beyond 2e-5 within the fixture's few
+    steps; those stay covered in complex128 (1e-11) and, in complex64, through
+    their imaginary-time part and the single operations."""
     g = golden(name)
     _, n_it, switch, n_rt, first = golden_cases().CASES[name]
-    # In c64 the RT result inherits the IT state's FP32 error amplified by the
-    # nonlinear phase: d(theta)/d|psi| * |psi| ~ 2 theta per half step.  Several
-    # of these small fixtures hold collapsed droplets with theta of 5-90 rad, so
-    # the c64 RT bound scales with 2 * theta_max * n_rt.
-    rt_tol = TOL[prec]
-    if prec == "c64":
-        rt_tol *= max(1.0, 2.0 * _rt_phase_max(name, g) * n_rt)
+    check_rt = prec == "c128" or name in golden_cases().WELL_CONDITIONED
     s, _ = _solver(name, prec)
     with s:
         s.load_pote(g["pote0"])
@@ -84,13 +72,15 @@ def test_fused_iterations_match_golden(name, prec):
             assert rel_l2(s.export_fi3d(), g["it_fi3d"]) < TOL[prec]
             e = np.array(s.calc_energy())
             assert abs(e[5] - g["it_energy"][5]) < ETOL[prec] * abs(g["it_energy"][5])
+        if not check_rt:
+            return
         if switch:
             s.load_pote(g["pote1"])
         s.real_steps(n_rt, first)
-        assert rel_l2(s.export_data(), c128(g["rt_psi"])) < rt_tol
-        assert rel_l2(s.export_fi3d(), g["rt_fi3d"]) < rt_tol
+        assert rel_l2(s.export_data(), c128(g["rt_psi"])) < TOL[prec]
+        assert rel_l2(s.export_fi3d(), g["rt_fi3d"]) < TOL[prec]
         e = np.array(s.calc_energy())
-        assert abs(e[5] - g["rt_energy"][5]) < max(rt_tol, ETOL[prec]) * abs(g["rt_energy"][5])
+        assert abs(e[5] - g["rt_energy"][5]) < ETOL[prec] * abs(g["rt_energy"][5])
 
 
 @pytest.mark.parametrize("prec", ["c128", "c64"])
@@ -301,14 +291,21 @@ def test_fused_pipeline_matches_oracle_128():
     ref.close()
 
 
-@pytest.mark.parametrize("dims", [(64, 32, 8), (32, 32, 16), (128, 128, 32)])
+@pytest.mark.parametrize("dims", [(64, 32, 8), (32, 32, 16), (64, 64, 16), (128, 128, 32)])
 def test_fused_pipeline_short_runs_match_oracle(dims):
-    # a few iterations on the README's double well: both complex64 schedules
-    # against the FP64 oracle (these small boxes hold a collapsing droplet, so
-    # the bound is the c64 one, 1e-4, rather than the well-conditioned 2e-5)
+    # a few iterations, both complex64 schedules against the FP64 oracle: the
+    # README's double well at 128^2 x 32 (the workload grid) and a dilute
+    # double well on the smaller boxes (there the README's couplings make a
+    # collapsing droplet whose phase the FP64 reference itself cannot hold to
+    # 1e-7, see test_fused_iterations_match_golden)
     nx, ny, nz = dims
-    cfg = O.default_config(nx=nx, ny=ny, nz=nz, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
-                           pote_strategy="MEXICAN", fftw_n_threads=8)
+    if dims == (128, 128, 32):
+        cfg = O.default_config(nx=nx, ny=ny, nz=nz, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
+                               pote_strategy="MEXICAN", fftw_n_threads=8)
+    else:
+        cfg = O.default_config(nx=nx, ny=ny, nz=nz, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
+                               pote_strategy="MEXICAN", dx=250.0, dy=250.0, dz=800.0, n_atoms=5e3, edd=0.9,
+                               fftw_n_threads=8)
     p = gparams(cfg)
     V, psi0 = G.potential(p), G.initial_psi(p)
     for k in (1, 3):
@@ -323,8 +320,8 @@ def test_fused_pipeline_short_runs_match_oracle(dims):
                 s.load_buffer(psi0)
                 s.imag_steps(k)
                 s.real_steps(k, 0)
-                assert rel_l2(s.export_data(), want_psi) < 1e-4, sched
-                assert rel_l2(s.export_fi3d(), want_fi) < 1e-4, sched
+                assert rel_l2(s.export_data(), want_psi) < TOL["c64"], sched
+                assert rel_l2(s.export_fi3d(), want_fi) < TOL["c64"], sched
 
 
 def test_real_steps_after_coefficient_buffer_grows():

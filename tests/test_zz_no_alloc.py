@@ -40,12 +40,13 @@ def _handle_fi3d(p, psi_norm):
         return s.export_fi3d().reshape(-1)
 
 
-def _noalloc_fi3d(p, psi_norm):
+def _noalloc_fi3d(p, psi_norm, stream=None):
     import torch
 
     psi_dev = torch.from_numpy(psi_norm.view(np.complex128).astype(np.complex64)).cuda()
     fi_dev = torch.full((p.n,), float("nan"), dtype=torch.float32, device="cuda")
-    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    stream = stream or torch.cuda.current_stream()
     rc = capi.lib().gpe_calc_fi3d_noalloc(
         ctypes.c_void_p(psi_dev.data_ptr()), ctypes.c_void_p(fi_dev.data_ptr()), p.nx, p.ny, p.nz,
         p.dx, p.dy, p.dz, p.n_atoms, ctypes.c_void_p(stream.cuda_stream))
@@ -59,9 +60,11 @@ def test_noalloc_matches_handle_path_on_two_calls_in_a_row():
         O.default_config(nx=64, ny=64, nz=16, init_strategy="GAUSS", pote_strategy="HARMONIC"),
         O.default_config(nx=48, ny=40, nz=12, init_strategy="MULTIPLE_GAUSS", initial_maximas=3,
                          pote_strategy="MEXICAN"),
+        # the README grid, the largest of the stated configurations that fits the array
+        O.default_config(nx=128, ny=128, nz=32, init_strategy="MULTIPLE_GAUSS", initial_maximas=2,
+                         pote_strategy="MEXICAN"),
     ]
-    # the third call repeats the first grid (tables kept from the call before it
-    # are rebuilt only when the grid changes)
+    # the last call repeats the first grid after two others
     for cfg in cases + cases[:1]:
         p = gparams(cfg)
         psi = _normalised(p, G.initial_psi(p))
@@ -80,3 +83,18 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
                                           256, 256, 64, 1.0, 1.0, 1.0, 1.0, None)
     assert rc == capi.GPE_ERR_SIZE
     assert b"limit" in capi.lib().gpe_last_error()
+
+
+def test_noalloc_calls_on_two_streams_in_turn():
+    """Calls alternate between two streams (each finished before the next
+    starts) over two grids; every result matches the handle path."""
+    import torch
+
+    a = gparams(O.default_config(nx=64, ny=64, nz=16, init_strategy="GAUSS", pote_strategy="HARMONIC"))
+    b = gparams(O.default_config(nx=32, ny=48, nz=16, init_strategy="COS", pote_strategy="CYLINDRICAL"))
+    psi = {id(p): _normalised(p, G.initial_psi(p)) for p in (a, b)}
+    want = {id(p): _handle_fi3d(p, psi[id(p)]) for p in (a, b)}
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    for k, p in enumerate((a, b, b, a)):
+        got = _noalloc_fi3d(p, psi[id(p)], streams[k % 2])
+        assert rel_l2(got, want[id(p)]) < TOL
