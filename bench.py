@@ -444,7 +444,8 @@ def run_our_arm(args):
             rc = L.gpe_time_kernel(solver.handle, idx, 200, ctypes.byref(ms), ctypes.byref(by))
             if rc != 0:
                 return False
-            kt[name] = (ms.value, by.value, L.gpe_kernel_name(idx).decode())
+            kname_ = solver.plane_kernel() if name == "F_YZ" else L.gpe_kernel_name(idx).decode()
+            kt[name] = (ms.value, by.value, kname_)
         return True
 
     if time_kernels(["F_YZ", "F_XK", "F_XD"]):

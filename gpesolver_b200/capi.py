@@ -114,6 +114,7 @@ SIGNATURES = [
     ("gpe_x_tiles", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("gpe_time_kernel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]),
     ("gpe_kernel_name", ctypes.c_char_p, [ctypes.c_int]),
+    ("gpe_plane_kernel_name", ctypes.c_char_p, [ctypes.c_void_p]),
     ("gpe_init_potential", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(gpe_init_params)]),
     ("gpe_init_psi", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(gpe_init_params)]),
     ("gpe_export_potential", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),

@@ -7,6 +7,7 @@
 // exported fields).
 #include "../../include/gpe_b200.h"
 #include "fused_yz.cuh"
+#include "plane_pair.cuh"
 #include "init.cuh"
 #include "kernels.cuh"
 #include "plan.hpp"
@@ -152,6 +153,7 @@ class SolverBase {
     virtual void it_batch_end()                              = 0;
     virtual const void *psi_ptr() const                      = 0;
     virtual void x_tiles(int *kin_lines, int *dip_lines) const  = 0;
+    virtual const char *plane_kernel() const                 = 0;
     virtual int device() const                               = 0;
 };
 
@@ -254,7 +256,9 @@ template <class R> class Solver final : public SolverBase {
             S2.alloc((size_t)nx * 2 * ny * nz);
             psir.alloc(N);
             GPE_CUDA(cudaMemsetAsync(psir.p, 0, sizeof(C) * N, cur)); // defined before any RT call
-            zpartial.alloc((size_t)(nx * ny + 31) / 32);
+            // per-CTA partial norms: one per 32 rows (four-kernel z pass), one per
+            // CTA of a plane kernel (2 nx with two CTAs per plane)
+            zpartial.alloc(std::max<size_t>((size_t)(nx * ny + 31) / 32, (size_t)2 * nx));
             ticket.alloc(1);
             build_vk2();
         }
@@ -263,6 +267,11 @@ template <class R> class Solver final : public SolverBase {
         GPE_CUDA(cudaStreamSynchronize(cur));
         set_smem_attrs();
         if (fused) {
+            // middle real- and imaginary-time iterations on the two-CTA plane
+            // kernels (k5_yz_pair, k5_yz_pair_it) unless GPE_PLANE_PAIR=0 keeps
+            // them on k4_yz
+            const char *pp = std::getenv("GPE_PLANE_PAIR");
+            plane_pair     = yz_plane() && !(pp && pp[0] == '0');
             set_fused_attrs();
             autotune_x();
         }
@@ -840,6 +849,8 @@ template <class R> class Solver final : public SolverBase {
         set((const void *)k4_yz<R, A, B, ZM_RT_EPI>, G::template smem<ZM_RT_EPI>());               \
         set((const void *)k4_yz<R, A, B, ZM_IT_PRO>, G::template smem<ZM_IT_PRO>());               \
         set((const void *)k4_yz<R, A, B, ZM_IT_MID>, G::template smem<ZM_IT_MID>());               \
+        set((const void *)k5_yz_pair<R, A, B>, PairShape<R, A, B>::SMEM);                          \
+        set((const void *)k5_yz_pair_it<R, A, B>, PairShapeIT<R, A, B>::SMEM);                     \
     }
             GPE_YZ_CASES(GPE_SETYZ)
 #undef GPE_SETYZ
@@ -1015,6 +1026,7 @@ template <class R> class Solver final : public SolverBase {
         *k = xk_lines;
         *d = xd_lines;
     }
+    const char *plane_kernel() const override { return plane_pair ? "k5_yz_pair" : (yz_plane() ? "k4_yz" : ""); }
 
     // Y pass (SIGN < 0 forward, > 0 inverse): kinetic lines (kin, part 0 or 1)
     // and dipolar lines (part 0, or !kin).  Tiles of 16 z columns (8 when nz = 8).
@@ -1095,7 +1107,14 @@ template <class R> class Solver final : public SolverBase {
 #define GPE_LYZ(A, B)                                                                              \
     if (ny == A && nz == B) {                                                                      \
         using G = YZShape<R, A, B>;                                                                \
-        launch(k4_yz<R, A, B, MODE>, nx, G::NT, G::template smem<MODE>(), s, a, t);               \
+        if (MODE == ZM_RT_MID && plane_pair)                                                       \
+            launch(k5_yz_pair<R, A, B>, 2 * nx, PairShape<R, A, B>::NT, PairShape<R, A, B>::SMEM,  \
+                   s, a, t);                                                                       \
+        else if (MODE == ZM_IT_MID && plane_pair)                                                  \
+            launch(k5_yz_pair_it<R, A, B>, 2 * nx, PairShape<R, A, B>::NT,                         \
+                   PairShapeIT<R, A, B>::SMEM, s, a, t);                                           \
+        else                                                                                       \
+            launch(k4_yz<R, A, B, MODE>, nx, G::NT, G::template smem<MODE>(), s, a, t);           \
     }
             GPE_YZ_CASES(GPE_LYZ)
 #undef GPE_LYZ
@@ -1272,6 +1291,7 @@ template <class R> class Solver final : public SolverBase {
     DevBuf<int> status, iter_zero, iter_base;
     // fused pipeline (compile-time line lengths; complex64 only)
     bool fused = false;
+    bool plane_pair = false; // middle iterations on the two-CTA plane kernels
     DevBuf<C> S2;
     DevBuf<C> psir; // real time: psi in real space after the last phase step
     int xk_lines = 16, xd_lines = 16; // x-pass lines per CTA (autotune_x)
@@ -2090,6 +2110,12 @@ const char *gpe_kernel_name(int which) {
     if (which < 0 || which >= GPE_K_COUNT)
         return "";
     return names[which];
+}
+
+const char *gpe_plane_kernel_name(gpe_handle *h) {
+    if (!h || !h->impl)
+        return "";
+    return h->impl->plane_kernel();
 }
 
 int gpe_launch_count(gpe_handle *h, long long *count) {

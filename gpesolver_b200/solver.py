@@ -133,6 +133,11 @@ class B200GrossPitaevskiSolver:
         capi.check(self._L.gpe_x_tiles(self._h, ctypes.byref(k), ctypes.byref(d)))
         return k.value, d.value
 
+    def plane_kernel(self) -> str:
+        """The plane kernel of the middle real-time iterations ("k5_yz_pair",
+        "k4_yz", or "" on grids without one)."""
+        return self._L.gpe_plane_kernel_name(self._h).decode()
+
     # -- data in / out (solver.cpp:118-131, gpu_solver.cpp:136-155) -------
     def load_buffer(self, psi) -> None:
         a = _as_c128_flat(psi, self.n)

@@ -193,6 +193,11 @@ int gpe_time_kernel(gpe_handle *h, int which, int reps, double *ms_per_launch,
                     double *bytes_per_launch);
 /* Name of kernel `which` as it appears in a profiler's launch list. */
 const char *gpe_kernel_name(int which);
+/* Name of the plane kernel that runs this handle's middle real-time iterations
+ * (GPE_K_F_YZ): "k5_yz_pair" (two CTAs per x plane; its imaginary-time
+ * counterpart is k5_yz_pair_it) or "k4_yz"; "" on grids without a plane
+ * kernel.  No reference counterpart. */
+const char *gpe_plane_kernel_name(gpe_handle *h);
 
 /* --- device-side initial state and potential --- */
 

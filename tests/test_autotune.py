@@ -6,7 +6,7 @@ import pytest
 
 import gpesolver_b200 as G
 
-from .helpers import WELL_CONDITIONED, gparams
+from .helpers import WELL_CONDITIONED, gparams, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -56,3 +56,29 @@ def test_y_column_choices_give_identical_results(monkeypatch):
             s.real_steps(20, 0)
             outs.append(s.export_data())
     np.testing.assert_array_equal(outs[1], outs[0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(32, 32, 16), (64, 64, 16), (64, 64, 32), (96, 96, 24), (128, 128, 32)])
+def test_plane_pair_kernel_matches_one_cta_plane_kernel(dims, monkeypatch):
+    """The middle imaginary- and real-time iterations on the two-CTA plane
+    kernels (k5_yz_pair_it, k5_yz_pair: one cluster per x plane) against the
+    one-CTA plane kernel (k4_yz): each line goes through the same radices,
+    twiddles and operations (only the norm's partial sums are grouped by half
+    planes), so psi and phi agree to rounding (1e-6)."""
+    p = gparams(WELL_CONDITIONED(*dims))
+    out = {}
+    for pair in ("1", "0"):
+        monkeypatch.setenv("GPE_PLANE_PAIR", pair)
+        with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
+            assert s.plane_kernel() == ("k5_yz_pair" if pair == "1" else "k4_yz")
+            s.load_pote(G.potential(p))
+            s.load_buffer(G.initial_psi(p))
+            s.imag_steps(20)
+            it = (s.export_data().copy(), s.export_fi3d().copy(), s.calc_norm())
+            s.real_steps(70, 0)
+            out[pair] = it + (s.export_data().copy(), s.export_fi3d().copy())
+    a, b = out["1"], out["0"]
+    assert rel_l2(a[0], b[0]) < 1e-6 and rel_l2(a[1], b[1]) < 1e-6
+    assert abs(a[2] - b[2]) < 1e-12 * abs(b[2])
+    assert rel_l2(a[3], b[3]) < 1e-6 and rel_l2(a[4], b[4]) < 1e-6
