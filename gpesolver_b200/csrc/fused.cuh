@@ -53,6 +53,23 @@ struct StepIdx {
 
 enum { ZM_RT_PRO = 0, ZM_RT_MID, ZM_RT_EPI, ZM_IT_PRO, ZM_IT_MID };
 
+// Asynchronous global -> shared copies (cp.async, completion per thread; a
+// barrier after the wait makes the data visible to the block).
+__device__ __forceinline__ void cp_async8(void *smem, const void *g) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *g) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most N of this thread's committed groups are pending
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+
 // ---------------------------------------------------------------------------
 // X pencils
 // ---------------------------------------------------------------------------
@@ -121,34 +138,63 @@ __global__ void __launch_bounds__(NT)
 // Dipolar x pencils: S(x, ky, kz) -> FFT_2nx (upper half zero) -> V_dd(k) * scale
 // -> iFFT_2nx, lower half kept.  scale = 1/(8N) (C2R normalisation) and, in
 // imaginary time, 1/xnorma (the spectrum was built from the unnormalised psi).
+// The twiddle table and the V_dd(k) values of the CTA's lines (|kx| = 0..nx) are
+// copied into shared memory (cp.async) at kernel start, behind the forward
+// transform's global loads, instead of being gathered from L2 after it.
+template <class R, int NX, int CNT> constexpr size_t x_dip_smem() {
+    return sizeof(cplx<R>) * (CNT * 2 * NX + 2 * NX) + sizeof(R) * (NX + 1) * CNT;
+}
+
 template <class R, int NX, int CNT, int NT>
 __global__ void __launch_bounds__(NT, NX >= 256 ? 2 : 3) // 512-point lines: two CTAs per SM; 256: three
     k3_x_dip(cplx<R> *__restrict__ S, const R *__restrict__ vk, const double *__restrict__ divisor,
              double dip_scale, int ny, int nz, Twid td) {
     using C          = cplx<R>;
     constexpr int L  = 2 * NX;
-    using Fw         = LinePass<-1, R, L, CNT, CNT, NT, false, false, true, false>;
-    using Iv         = LinePass<+1, R, L, CNT, CNT, NT, false, true, false, true>;
+    // two-stage lines (radix pairs) take their twiddles from the shared copy;
+    // longer radix chains (nx = 96) keep the global table in the middle stages
+    constexpr bool TW2 = radices_of(L).n == 2;
+    using Fw         = LinePass<-1, R, L, CNT, CNT, NT, false, false, true, false, TW2>;
+    using Iv         = LinePass<+1, R, L, CNT, CNT, NT, false, true, false, true, TW2>;
     static_assert(Fw::RL == Iv::R0 && Fw::ROUNDSL == Iv::ROUNDS0 && Fw::ITEMSL == Iv::ITEMS0,
                   "paired transforms share the register layout");
     const int tid  = threadIdx.x;
     C *buf         = reinterpret_cast<C *>(g_smem);
-    const C *tw    = (const C *)td.tw, *tl = (const C *)td.lo;
+    C *tws         = buf + CNT * L;                    // twiddles exp(-2 pi i m / L)
+    R *vs          = reinterpret_cast<R *>(tws + L);   // V_dd of |kx| = 0..NX, line b: vs[|kx| CNT + b]
+    const C *tw    = (const C *)td.tw;
+    const C *twu   = TW2 ? tws : tw;                   // the table the stages read
     const int cols = 2 * ny * nz;
     const int c0   = blockIdx.x * CNT;
     const int cnt  = min(CNT, cols - c0);
+    const size_t xs = (size_t)(ny + 1) * nz;
+    for (int m = tid; m < L; m += NT)
+        cp_async8(&tws[m], &tw[m]);
+    for (int e = tid; e < (NX + 1) * CNT; e += NT) {
+        const int ix = e / CNT, b = e - ix * CNT;
+        const int c  = min(c0 + b, cols - 1);
+        const int ky = c / nz, kz = c - ky * nz;
+        const int iy = ky <= ny ? ky : 2 * ny - ky;
+        cp_async4(&vs[e], &vk[(size_t)ix * xs + (size_t)iy * nz + kz]);
+    }
+    cp_async_commit();
+    auto ld = [&](int b, int t) { return b < cnt ? S[(size_t)t * cols + c0 + b] : C{(R)0, (R)0}; };
     C a[Fw::ROUNDSL][Fw::RL];
-    Fw::run_to_regs(
-        buf, [&](int b, int t) { return b < cnt ? S[(size_t)t * cols + c0 + b] : C{(R)0, (R)0}; }, a, tw, tl,
-        tid);
+    Fw::stage0_to_tile(buf, ld, tid);
+    cp_async_wait<0>();
+    __syncthreads();
+    Fw::template middle<1>(buf, twu, nullptr, tid);
+#pragma unroll
+    for (int rd = 0; rd < Fw::ROUNDSL; ++rd) {
+        const int it = rd * NT + tid;
+        if (!Fw::template valid<Fw::ITEMSL>(it))
+            break;
+        const int j = it / CNT, b = it - j * CNT;
+        Fw::loadL(buf, a[rd], j, b, twu, nullptr);
+    }
     {
         const R scale = (R)(divisor ? dip_scale / divisor[0] : dip_scale);
         const int b   = Fw::line_of(tid);
-        const int c   = min(c0 + b, cols - 1);
-        const int ky = c / nz, kz = c - ky * nz;
-        const int iy      = ky <= ny ? ky : 2 * ny - ky;
-        const R *vcol     = vk + (size_t)iy * nz + kz; // + ix * (ny+1) * nz
-        const size_t xs   = (size_t)(ny + 1) * nz;
 #pragma unroll
         for (int rd = 0; rd < Fw::ROUNDSL; ++rd) {
             if (!Fw::template valid<Fw::ITEMSL>(rd * NT + tid))
@@ -157,7 +203,7 @@ __global__ void __launch_bounds__(NT, NX >= 256 ? 2 : 3) // 512-point lines: two
             for (int q = 0; q < Fw::RL; ++q) {
                 const int t  = Fw::last_index(tid, rd, q);
                 const int ix = t <= NX ? t : L - t;
-                a[rd][q]     = cscale(a[rd][q], __ldg(&vcol[ix * xs]) * scale);
+                a[rd][q]     = cscale(a[rd][q], vs[ix * CNT + b] * scale);
             }
         }
     }
@@ -168,7 +214,7 @@ __global__ void __launch_bounds__(NT, NX >= 256 ? 2 : 3) // 512-point lines: two
             if (b < cnt)
                 S[(size_t)t * cols + c0 + b] = v;
         },
-        tw, tl, tid);
+        twu, nullptr, tid);
 }
 
 // ---------------------------------------------------------------------------
@@ -244,22 +290,6 @@ struct ZArgs {
     double cx, cy, cz, dtau; // IT stencil
     int nx, ny;
 };
-
-// Asynchronous global -> shared copies (cp.async, completion per thread; a
-// barrier after the wait makes the data visible to the block).
-__device__ __forceinline__ void cp_async8(void *smem, const void *g) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void *smem, const void *g) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// wait until at most N of this thread's committed groups are pending
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 template <class R, int NZ, int MODE>
 __global__ void __launch_bounds__(256, 4) k2_z(ZArgs a, Twid tk, Twid td) {

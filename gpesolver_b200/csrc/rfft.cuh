@@ -35,8 +35,10 @@ __host__ __device__ constexpr Radices reversed(Radices r) {
     return o;
 }
 
+// TWS: the twiddle table passed to the stages is in shared memory (plain loads
+// instead of read-only global loads).
 template <int SIGN, class R, int L, int COUNT, int TS, int NT, bool CMP, bool REV, bool IH = false,
-          bool OH = false>
+          bool OH = false, bool TWS = false>
 struct LinePass {
     using C                        = cplx<R>;
     static constexpr Radices RAD   = REV ? reversed(radices_of(L)) : radices_of(L);
@@ -75,9 +77,9 @@ struct LinePass {
     static __device__ __forceinline__ void twiddle(C &v, int jm, int k, int NS, int STEP, const C *tw,
                                                    const C *twlo) {
         const int t = jm * k * STEP;
-        const C w   = __ldg(&tw[t]);
+        const C w   = TWS ? tw[t] : __ldg(&tw[t]);
         if constexpr (sizeof(R) == 4 && CMP)
-            v = twmul<SIGN>(v, w, __ldg(&twlo[t]));
+            v = twmul<SIGN>(v, w, TWS ? twlo[t] : __ldg(&twlo[t]));
         else
             v = SIGN < 0 ? cmul(v, w) : cmulc(v, w);
     }

@@ -75,6 +75,15 @@ __global__ void __launch_bounds__(256)
 
 __global__ void k_advance(int *counter, int by) { counter[0] += by; }
 
+// Device-side loop of a batch graph (a while node around one chunk of
+// iterations): the counter is set before the loop and counted down at the end
+// of every pass; the pass that reaches zero ends the loop.
+__global__ void k_loop_init(int *counter, int passes) { counter[0] = passes; }
+__global__ void k_loop_step(int *counter, cudaGraphConditionalHandle loop) {
+    if (--counter[0] <= 0)
+        cudaGraphSetConditional(loop, 0);
+}
+
 __global__ void k_set_f64(double *p, double v) { p[0] = v; }
 
 // ---------------------------------------------------------------------------
@@ -869,7 +878,7 @@ template <class R> class Solver final : public SolverBase {
     // x-pass launches for nx = NN with CNT lines per CTA (the autotuned choice)
     template <int NN, int CNT, class Set> static void set_x_attrs(Set &set) {
         set((const void *)k3_x_kin<R, NN, CNT, pass_threads<NN, CNT>()>, xy_smem<R, NN, CNT>());
-        set((const void *)k3_x_dip<R, NN, CNT, pass_threads<2 * NN, CNT>()>, xy_smem<R, 2 * NN, CNT>());
+        set((const void *)k3_x_dip<R, NN, CNT, pass_threads<2 * NN, CNT>()>, x_dip_smem<R, NN, CNT>());
     }
     template <int NN, int CNT> void launch_xk(cudaStream_t s) {
         constexpr int NT = pass_threads<NN, CNT>();
@@ -878,7 +887,7 @@ template <class R> class Solver final : public SolverBase {
     }
     template <int NN, int CNT> void launch_xd(cudaStream_t s, const double *divisor, double dscale) {
         constexpr int NT = pass_threads<2 * NN, CNT>();
-        launch(k3_x_dip<R, NN, CNT, NT>, (2 * ny * nz + CNT - 1) / CNT, NT, xy_smem<R, 2 * NN, CNT>(), s, S2.p,
+        launch(k3_x_dip<R, NN, CNT, NT>, (2 * ny * nz + CNT - 1) / CNT, NT, x_dip_smem<R, NN, CNT>(), s, S2.p,
                (const R *)vk2.p, divisor, dscale, ny, nz, twid(dx));
     }
     template <int NN> void f_x_n(cudaStream_t s, bool kin, const double *divisor, int part, double dscale) {
@@ -1692,12 +1701,17 @@ struct gpe_batch {
     cudaStream_t own    = nullptr; // the batch's own stream
     cudaStream_t cur    = nullptr;
     cudaStream_t root   = nullptr; // capture origin
+    cudaStream_t body   = nullptr; // capture origin of the loop body
     cudaEvent_t fork    = nullptr;
+    int *loop_counter   = nullptr; // device counter of the loop's passes
+    static constexpr int kChunk = 64; // iterations per pass of the loop body
     struct Graph {
         cudaGraphExec_t exec = nullptr;
-        std::vector<long long> nodes; // kernel launches per member
+        std::vector<long long> pro, chunk, rest; // kernel launches per member of each piece
+        long passes = 0;
+        int rem     = 0;
     };
-    std::map<std::tuple<int, int, std::vector<const void *>>, Graph> graphs;
+    std::map<std::tuple<long, std::vector<const void *>>, Graph> graphs;
 
     ~gpe_batch() {
         cudaSetDevice(device);
@@ -1707,29 +1721,78 @@ struct gpe_batch {
             cudaGraphExecDestroy(kv.second.exec);
         for (auto *m : members)
             delete m;
+        if (loop_counter)
+            cudaFree(loop_counter);
         if (fork)
             cudaEventDestroy(fork);
+        if (body)
+            cudaStreamDestroy(body);
         if (root)
             cudaStreamDestroy(root);
         if (own)
             cudaStreamDestroy(own);
     }
 
-    // One launch of the batch graph for (kind, count): kind 20 the IT prologue,
-    // 21 `count` IT iterations of every member.
-    void run(int kind, int count) {
+    // Every member's piece (kind 20: prologue, 21: `count` iterations) as one
+    // graph branch each, forked from and joined to `origin`.
+    std::vector<long long> branches(int kind, int count, cudaStream_t origin) {
+        std::vector<long long> nodes;
+        GPE_CUDA(cudaEventRecord(fork, origin));
+        for (auto *m : members)
+            nodes.push_back(m->impl->capture_it_branch(kind, count, fork, origin));
+        return nodes;
+    }
+
+    // k imaginary-time iterations of every member as ONE graph launch: the
+    // prologue, a while node whose body runs kChunk iterations of every member
+    // (k / kChunk passes, counted on the device), then the remaining k % kChunk
+    // iterations.
+    void run(long k) {
         std::vector<const void *> sig;
         for (auto *m : members)
             sig.push_back(m->impl->psi_ptr());
-        auto key = std::make_tuple(kind, count, sig);
+        auto key = std::make_tuple(k, sig);
         auto it  = graphs.find(key);
         if (it == graphs.end()) {
             Graph g;
+            g.passes = k / kChunk;
+            g.rem    = (int)(k % kChunk);
             GPE_CUDA(cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal));
             try {
-                GPE_CUDA(cudaEventRecord(fork, root));
-                for (auto *m : members)
-                    g.nodes.push_back(m->impl->capture_it_branch(kind, count, fork, root));
+                g.pro = branches(20, 0, root);
+                if (g.passes > 0) {
+                    gpe::k_loop_init<<<1, 1, 0, root>>>(loop_counter, (int)g.passes);
+                    GPE_CUDA(cudaGetLastError());
+                    cudaStreamCaptureStatus st;
+                    cudaGraph_t graph         = nullptr;
+                    const cudaGraphNode_t *dp = nullptr;
+                    size_t nd                 = 0;
+                    GPE_CUDA(cudaStreamGetCaptureInfo(root, &st, nullptr, &graph, &dp, &nd));
+                    cudaGraphConditionalHandle loop;
+                    GPE_CUDA(cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault));
+                    cudaGraphNodeParams cp = {};
+                    cp.type                = cudaGraphNodeTypeConditional;
+                    cp.conditional.handle  = loop;
+                    cp.conditional.type    = cudaGraphCondTypeWhile;
+                    cp.conditional.size    = 1;
+                    cudaGraphNode_t cnode;
+                    GPE_CUDA(cudaGraphAddNode(&cnode, graph, dp, nd, &cp));
+                    GPE_CUDA(cudaStreamUpdateCaptureDependencies(root, &cnode, 1, cudaStreamSetCaptureDependencies));
+                    cudaGraph_t bg = cp.conditional.phGraph_out[0];
+                    GPE_CUDA(cudaStreamBeginCaptureToGraph(body, bg, nullptr, nullptr, 0,
+                                                           cudaStreamCaptureModeThreadLocal));
+                    try {
+                        g.chunk = branches(21, kChunk, body);
+                        gpe::k_loop_step<<<1, 1, 0, body>>>(loop_counter, loop);
+                        GPE_CUDA(cudaGetLastError());
+                    } catch (...) {
+                        cudaStreamEndCapture(body, &bg);
+                        throw;
+                    }
+                    GPE_CUDA(cudaStreamEndCapture(body, &bg));
+                }
+                if (g.rem > 0)
+                    g.rest = branches(21, g.rem, root);
             } catch (...) {
                 cudaGraph_t gr = nullptr;
                 cudaStreamEndCapture(root, &gr);
@@ -1743,9 +1806,15 @@ struct gpe_batch {
             cudaGraphDestroy(gr);
             it = graphs.emplace(key, std::move(g)).first;
         }
-        GPE_CUDA(cudaGraphLaunch(it->second.exec, cur));
-        for (size_t m = 0; m < members.size(); ++m)
-            members[m]->impl->it_batch_after(kind, count, it->second.nodes[m]);
+        const Graph &g = it->second;
+        GPE_CUDA(cudaGraphLaunch(g.exec, cur));
+        for (size_t m = 0; m < members.size(); ++m) {
+            members[m]->impl->it_batch_after(20, 0, g.pro[m]);
+            for (long p = 0; p < g.passes; ++p)
+                members[m]->impl->it_batch_after(21, kChunk, g.chunk[m]);
+            if (g.rem > 0)
+                members[m]->impl->it_batch_after(21, g.rem, g.rest[m]);
+        }
     }
 };
 
@@ -1896,7 +1965,9 @@ int gpe_batch_create(const gpe_params *members, int count, gpe_batch **out) {
         GPE_CUDA(cudaSetDevice(b->device));
         GPE_CUDA(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking));
         GPE_CUDA(cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking));
+        GPE_CUDA(cudaStreamCreateWithFlags(&b->body, cudaStreamNonBlocking));
         GPE_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        GPE_CUDA(cudaMalloc(&b->loop_counter, sizeof(int)));
         b->cur = b->own;
         for (int m = 0; m < count; ++m) {
             gpe_handle *h = nullptr;
@@ -1949,17 +2020,9 @@ int gpe_batch_imag_steps(gpe_batch *b, long k) {
     return guarded([&] {
         for (auto *m : b->members)
             m->impl->it_batch_begin();
-        // the fused imaginary-time schedule of every member (fused_imag):
-        // prologue, chunks of 64 iterations, remainder
-        b->run(20, 0);
-        constexpr int CH = 64;
-        long done        = 0;
-        while (k - done >= CH) {
-            b->run(21, CH);
-            done += CH;
-        }
-        if (k - done > 0)
-            b->run(21, (int)(k - done));
+        // the fused imaginary-time schedule of every member (fused_imag:
+        // prologue, chunks of 64 iterations, remainder) in one graph launch
+        b->run(k);
         for (auto *m : b->members)
             m->impl->it_batch_end();
     });
