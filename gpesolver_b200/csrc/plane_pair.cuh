@@ -316,25 +316,42 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairShape<R, NY, NZ>
             break;
         DFT<ZF::First::RADIX, -1, R, true>::run(zr[rd]);
     }
-    ZF::First::write(ZK, zr, tid);
-    __syncthreads();
-    plane_out<R, NYH, NZ, PZ, NT>(Pr_g, RP, tid); // kept psi for the next iteration
-    joint_stages<R2C, 0, R2C::NSTG, ZF, 1, ZF::NSTG - 1>(DP, dzt, dzl, ZK, kzt, kzl, tid);
-    {
-        // last FFT_z stage: bin kz of row y goes to the CTA owning column kz
+    // bin kz of row y of the finished FFT_z goes to the CTA owning column kz
+    // (XK's lower part: nothing reads it between the two cluster barriers)
+    auto emit_kz = [&](const auto &v, int rd, int line, auto elem) {
+        const int yg = y0 + line;
+#pragma unroll
+        for (int q = 0; q < (int)(sizeof(v[0]) / sizeof(v[0][0])); ++q) {
+            const int kz = elem(q);
+            C *d         = ((kz >= NZH) == (r == 1)) ? XK : XKo;
+            d[yg * PC + (kz % NZH)] = v[rd][q];
+        }
+    };
+    if constexpr (ZF::NSTG == 1) {
+        // a single-stage z transform (nz = 16) is finished in the registers
+#pragma unroll
+        for (int rd = 0; rd < ZF::First::ROUNDS; ++rd) {
+            if (!ZF::First::valid(rd * NT + tid))
+                break;
+            emit_kz(zr, rd, ZF::First::line(tid, rd), [&](int q) { return ZF::First::elem(tid, rd, q); });
+        }
+        __syncthreads(); // DP (R2C pair lines) complete
+        plane_out<R, NYH, NZ, PZ, NT>(Pr_g, RP, tid); // kept psi for the next iteration
+        R2C::template stages<0, R2C::NSTG>(DP, dzt, dzl, tid);
+        pair_unpack_r2c<R, NY, NZ, NT>(XD, XDo, DP, r, tid);
+    } else {
+        ZF::First::write(ZK, zr, tid);
+        __syncthreads();
+        plane_out<R, NYH, NZ, PZ, NT>(Pr_g, RP, tid); // kept psi for the next iteration
+        joint_stages<R2C, 0, R2C::NSTG, ZF, 1, ZF::NSTG - 1>(DP, dzt, dzl, ZK, kzt, kzl, tid);
+        // last FFT_z stage, emitted to the column owners
         typename ZF::Last::Regs fa;
         ZF::Last::read(ZK, fa, kzt, kzl, tid);
 #pragma unroll
         for (int rd = 0; rd < ZF::Last::ROUNDS; ++rd) {
             if (!ZF::Last::valid(rd * NT + tid))
                 break;
-            const int yg = y0 + ZF::Last::line(tid, rd);
-#pragma unroll
-            for (int q = 0; q < ZF::Last::RADIX; ++q) {
-                const int kz = ZF::Last::elem(tid, rd, q);
-                C *d         = ((kz >= NZH) == (r == 1)) ? XK : XKo;
-                d[yg * PC + (kz % NZH)] = fa[rd][q];
-            }
+            emit_kz(fa, rd, ZF::Last::line(tid, rd), [&](int q) { return ZF::Last::elem(tid, rd, q); });
         }
         pair_unpack_r2c<R, NY, NZ, NT>(XD, XDo, DP, r, tid);
     }

@@ -173,14 +173,21 @@ class WarmStartNet:
                                                      self.n_voxels))
 
 
-def ground_states(params: Sequence[PhysicalParameters], iters: int, batch: int = 64, device: int = 0):
+def ground_states(params: Sequence[PhysicalParameters], iters: int, batch: int = 64, device: int = 0,
+                  converge_tol: float | None = None, max_chunks: int = 8):
     """Amplitude targets (torch float32 on the device, one row per solve,
-    scaled by target_scale) after `iters` imaginary-time iterations of each
-    solve from its Gaussian start, batched."""
+    scaled by target_scale) after imaginary time from each solve's Gaussian
+    start, batched.  With converge_tol, every batch keeps stepping in chunks of
+    `iters` iterations (at most max_chunks) until the total energy of every
+    member changes by less than converge_tol (relative) over a chunk, so that
+    the targets are ground states and not states still relaxing; without it,
+    each member runs `iters` iterations.  Returns (targets, chunks run per
+    batch)."""
     import torch
 
     n = params[0].n
     out = torch.empty((len(params), n), dtype=torch.float32, device=f"cuda:{device}")
+    chunks = []
     for s in range(0, len(params), batch):
         chunk = params[s:s + batch]
         with B200Batch(chunk, device) as b:
@@ -188,11 +195,23 @@ def ground_states(params: Sequence[PhysicalParameters], iters: int, batch: int =
                 m.init_pote()
                 m.init_buffer("GAUSS")
             b.imag_steps(iters)
+            done = 1
+            if converge_tol is not None:
+                e_prev = np.array([m.calc_energy().e_total for m in b.members])
+                while done < max_chunks:
+                    b.imag_steps(iters)
+                    done += 1
+                    e = np.array([m.calc_energy().e_total for m in b.members])
+                    worst = float(np.max(np.abs(e - e_prev) / np.abs(e)))
+                    e_prev = e
+                    if worst < converge_tol:
+                        break
+            chunks.append(done)
             for r, m in enumerate(b.members):
                 row = out[s + r]
                 capi.check(capi.lib().gpe_export_amplitude_device(m.handle, ctypes.c_void_p(row.data_ptr()), n))
                 row.mul_(target_scale(m.params))
-    return out
+    return out, chunks
 
 
 def train(net: WarmStartNet, params: Sequence[PhysicalParameters], targets, epochs: int, batch: int,

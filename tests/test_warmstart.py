@@ -50,7 +50,7 @@ def test_trained_network_shortens_imaginary_time():
     grids = ((64, 64, 16),)
     train_p = sweep.sweep_params(count=128, seed=11, grids=grids)
     held_p = sweep.sweep_params(count=6, seed=12, grids=grids)
-    targets = W.ground_states(train_p, iters=3000)
+    targets, _ = W.ground_states(train_p, iters=3000)
     cfg = W.WarmConfig(nx=64, ny=64, nz=16, levels=3, channels=(16, 16, 8, 4), hidden=64, max_batch=8)
     net = W.WarmStartNet(cfg, seed=1)
     hist = W.train(net, train_p, targets, epochs=40, batch=8, lr=1e-3, lr_final=3e-5)
