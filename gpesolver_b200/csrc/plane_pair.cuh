@@ -71,8 +71,11 @@ template <class R, int NY, int NZ> struct PairShape {
     static constexpr size_t SMEM   = OFF_FP + sizeof(R) * FPN;
     static_assert(NZ % 4 == 0 && NY % 4 == 0, "halves of even row pairs and columns");
     static_assert(sizeof(C) * TD * LD <= XD_B - OFF_DP, "DP fits in the upper half of XD");
+    // half the one-CTA kernel's threads, at least 128, whole warps (the norm
+    // reduction of k5_yz_pair_it shuffles over full warps)
     static constexpr int NT0 = YZShape<R, NY, NZ>::NT / 2;
-    static constexpr int NT  = NT0 < 128 ? 128 : NT0;
+    static constexpr int NT  = NT0 < 128 ? 128 : (NT0 + 31) / 32 * 32;
+    static_assert(NT % 32 == 0, "whole warps");
     static __device__ __forceinline__ int fpi(int r, int k) { return (r & 1) * FH + (r >> 1) * FS + k; }
 };
 
