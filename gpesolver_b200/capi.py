@@ -96,6 +96,7 @@ SIGNATURES = [
     ("gpe_load_potential", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     ("gpe_export_psi", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     ("gpe_export_fi3d", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
+    ("gpe_load_fi3d", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     ("gpe_export_psi_async", ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_size_t]),
     ("gpe_export_wait", ctypes.c_int, [ctypes.c_void_p]),
     ("gpe_calc_fi3d", ctypes.c_int, [ctypes.c_void_p]),

@@ -141,12 +141,14 @@ class Checkpointer:
     def _flush(self):
         if self._pending is None:
             return
-        buf, name, meta = self._pending
+        buf, name, meta, fi3d = self._pending
         self.solver.export_wait()
         psi = buf.view(np.complex128)
 
         def write():
             save_binary(psi, self.solver.params, name)
+            if fi3d is not None:
+                fi3d.tofile(meta["fi3d_file"])
             with open(name + ".resume.json", "w") as f:
                 json.dump(meta, f)
 
@@ -164,8 +166,15 @@ class Checkpointer:
         self.solver.export_async(buf)
         name = f"{self.prefix}_{self.counter}"
         self.counter += 1
-        self._pending = (buf, name, {"phase": phase, "iteration": int(iteration),
-                                     "edd": float(self.solver.params.edd), "file": name + BINARY_EXT})
+        meta = {"phase": phase, "iteration": int(iteration), "edd": float(self.solver.params.edd),
+                "file": name + BINARY_EXT}
+        fi3d = None
+        if phase == "real":
+            # the field the next real-time iteration's first half step uses
+            # (raw FP64, nx*ny*nz values), for an exact resume
+            fi3d = self.solver.export_fi3d().reshape(-1)
+            meta["fi3d_file"] = name + ".fi3d.f64"
+        self._pending = (buf, name, meta, fi3d)
 
     def close(self) -> None:
         self._flush()

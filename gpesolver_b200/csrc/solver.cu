@@ -75,15 +75,6 @@ __global__ void __launch_bounds__(256)
 
 __global__ void k_advance(int *counter, int by) { counter[0] += by; }
 
-// Device-side loop of a batch graph (a while node around one chunk of
-// iterations): the counter is set before the loop and counted down at the end
-// of every pass; the pass that reaches zero ends the loop.
-__global__ void k_loop_init(int *counter, int passes) { counter[0] = passes; }
-__global__ void k_loop_step(int *counter, cudaGraphConditionalHandle loop) {
-    if (--counter[0] <= 0)
-        cudaGraphSetConditional(loop, 0);
-}
-
 __global__ void k_set_f64(double *p, double v) { p[0] = v; }
 
 // ---------------------------------------------------------------------------
@@ -129,6 +120,7 @@ class SolverBase {
     virtual void load_potential(const double *V)             = 0;
     virtual void export_psi(double *out)                     = 0;
     virtual void export_fi3d(double *out)                    = 0;
+    virtual void load_fi3d(const double *fi3d)               = 0;
     virtual void calc_fi3d()                                 = 0;
     virtual void imag_linear()                               = 0;
     virtual void imag_nonlinear()                            = 0;
@@ -276,11 +268,6 @@ template <class R> class Solver final : public SolverBase {
         GPE_CUDA(cudaStreamSynchronize(cur));
         set_smem_attrs();
         if (fused) {
-            // middle real- and imaginary-time iterations on the two-CTA plane
-            // kernels (k5_yz_pair, k5_yz_pair_it) unless GPE_PLANE_PAIR=0 keeps
-            // them on k4_yz
-            const char *pp = std::getenv("GPE_PLANE_PAIR");
-            plane_pair     = yz_plane() && !(pp && pp[0] == '0');
             set_fused_attrs();
             autotune_x();
         }
@@ -450,6 +437,12 @@ template <class R> class Solver final : public SolverBase {
         launch(k_to_f64<R>, grid_elem(N), 256, 0, cur, (const R *)phi.p, staging.p, N,
                (const double *)one_ptr(), 1);
         GPE_CUDA(cudaMemcpyAsync(h, staging.p, sizeof(double) * N, cudaMemcpyDeviceToHost, cur));
+        GPE_CUDA(cudaStreamSynchronize(cur));
+    }
+
+    void load_fi3d(const double *h) override {
+        GPE_CUDA(cudaMemcpyAsync(staging.p, h, sizeof(double) * N, cudaMemcpyHostToDevice, cur));
+        launch(k_from_f64<R>, grid_elem(N), 256, 0, cur, (const double *)staging.p, phi.p, N);
         GPE_CUDA(cudaStreamSynchronize(cur));
     }
 
@@ -924,7 +917,14 @@ template <class R> class Solver final : public SolverBase {
     // 16) fix them.
     void autotune_x() {
         y_lines = nz >= 16 ? 16 : 8;
-        bool fix_x = false, fix_y = false;
+        bool fix_x = false, fix_y = false, fix_p = false;
+        if (const char *env = std::getenv("GPE_PLANE_PAIR")) {
+            if (env[0] == '0' || env[0] == '1') {
+                pair_rt = pair_it = yz_plane() && env[0] == '1';
+                fix_p             = true;
+            }
+        }
+        const bool tune_p = yz_plane() && !fix_p;
         if (const char *env = std::getenv("GPE_X_TILES")) {
             int k = 0, d = 0;
             if (std::sscanf(env, "%d,%d", &k, &d) == 2 && (k == 8 || k == 16) && (d == 8 || d == 16)) {
@@ -941,12 +941,12 @@ template <class R> class Solver final : public SolverBase {
             }
         }
         const bool tune_y = !fix_y && !yz_plane() && nz >= 16;
-        if (fix_x && !tune_y)
+        if (fix_x && !tune_y && !tune_p)
             return;
         static std::mutex mu;
         // keyed by the schedule too: the plane schedule never tunes y_lines, so a
         // four-kernel solver of the same grid must not reuse its untuned value
-        static std::map<std::tuple<int, int, int, int, bool>, std::tuple<int, int, int>> chosen;
+        static std::map<std::tuple<int, int, int, int, bool>, std::tuple<int, int, int, int>> chosen;
         const auto key = std::make_tuple(P.device, nx, ny, nz, yz_plane());
         std::lock_guard<std::mutex> lock(mu);
         const auto it = chosen.find(key);
@@ -957,6 +957,10 @@ template <class R> class Solver final : public SolverBase {
             }
             if (tune_y)
                 y_lines = std::get<2>(it->second);
+            if (tune_p) {
+                pair_rt = (std::get<3>(it->second) & 1) != 0;
+                pair_it = (std::get<3>(it->second) & 2) != 0;
+            }
             return;
         }
         GPE_CUDA(cudaMemsetAsync(psi.p, 0, sizeof(C) * N, cur));
@@ -1023,19 +1027,43 @@ template <class R> class Solver final : public SolverBase {
                 }
             }
         }
+        if (tune_p) {
+            // the plane kernel of the middle iterations: one CTA per x plane
+            // (k4_yz) or a two-CTA cluster per plane (k5_yz_pair[_it]), each
+            // timed on the zeroed fields with a zero coefficient table; the
+            // imaginary-time launches leave a zero norm behind, which is reset
+            DevBuf<StepCoef> tcoef;
+            tcoef.alloc(2);
+            GPE_CUDA(cudaMemsetAsync(tcoef.p, 0, sizeof(StepCoef) * 2, cur));
+            GPE_CUDA(cudaMemsetAsync(iter_base.p, 0, sizeof(int), cur));
+            float trt[2], tit[2];
+            for (int v = 0; v < 2; ++v) {
+                pair_rt = pair_it = v == 1;
+                trt[v]  = time_of([&] { f_yz<ZM_RT_MID>(cur, psi.p, psi.p, tcoef.p, 0); });
+                tit[v]  = time_of([&] { f_yz<ZM_IT_MID>(cur, psi.p, psii.p, tcoef.p, 0); });
+            }
+            GPE_CUDA(cudaStreamSynchronize(cur));
+            // the pair replaces the one-CTA kernel only when 3% faster
+            pair_rt = trt[1] < 0.97f * trt[0];
+            pair_it = tit[1] < 0.97f * tit[0];
+            GPE_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int) * 4, cur));
+            GPE_CUDA(cudaMemcpyAsync(norm_state.p, one_buf.p, sizeof(double), cudaMemcpyDeviceToDevice, cur));
+            set_divisor_one();
+            GPE_CUDA(cudaStreamSynchronize(cur));
+        }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         xk_lines = best_k;
         xd_lines = best_d;
         y_lines  = best_y;
-        if (!fix_x && !fix_y) // only measured choices are shared
-            chosen[key] = std::make_tuple(best_k, best_d, best_y);
+        if (!fix_x && !fix_y && !fix_p) // only measured choices are shared
+            chosen[key] = std::make_tuple(best_k, best_d, best_y, (pair_rt ? 1 : 0) | (pair_it ? 2 : 0));
     }
     void x_tiles(int *k, int *d) const override {
         *k = xk_lines;
         *d = xd_lines;
     }
-    const char *plane_kernel() const override { return plane_pair ? "k5_yz_pair" : (yz_plane() ? "k4_yz" : ""); }
+    const char *plane_kernel() const override { return pair_rt ? "k5_yz_pair" : (yz_plane() ? "k4_yz" : ""); }
 
     // Y pass (SIGN < 0 forward, > 0 inverse): kinetic lines (kin, part 0 or 1)
     // and dipolar lines (part 0, or !kin).  Tiles of 16 z columns (8 when nz = 8).
@@ -1116,10 +1144,10 @@ template <class R> class Solver final : public SolverBase {
 #define GPE_LYZ(A, B)                                                                              \
     if (ny == A && nz == B) {                                                                      \
         using G = YZShape<R, A, B>;                                                                \
-        if (MODE == ZM_RT_MID && plane_pair)                                                       \
+        if (MODE == ZM_RT_MID && pair_rt)                                                          \
             launch(k5_yz_pair<R, A, B>, 2 * nx, PairShape<R, A, B>::NT, PairShape<R, A, B>::SMEM,  \
                    s, a, t);                                                                       \
-        else if (MODE == ZM_IT_MID && plane_pair)                                                  \
+        else if (MODE == ZM_IT_MID && pair_it)                                                     \
             launch(k5_yz_pair_it<R, A, B>, 2 * nx, PairShape<R, A, B>::NT,                         \
                    PairShapeIT<R, A, B>::SMEM, s, a, t);                                           \
         else                                                                                       \
@@ -1300,7 +1328,9 @@ template <class R> class Solver final : public SolverBase {
     DevBuf<int> status, iter_zero, iter_base;
     // fused pipeline (compile-time line lengths; complex64 only)
     bool fused = false;
-    bool plane_pair = false; // middle iterations on the two-CTA plane kernels
+    // middle real- / imaginary-time iterations on the two-CTA plane kernels
+    // (k5_yz_pair, k5_yz_pair_it) instead of k4_yz: picked by autotune_x
+    bool pair_rt = false, pair_it = false;
     DevBuf<C> S2;
     DevBuf<C> psir; // real time: psi in real space after the last phase step
     int xk_lines = 16, xd_lines = 16; // x-pass lines per CTA (autotune_x)
@@ -1701,17 +1731,12 @@ struct gpe_batch {
     cudaStream_t own    = nullptr; // the batch's own stream
     cudaStream_t cur    = nullptr;
     cudaStream_t root   = nullptr; // capture origin
-    cudaStream_t body   = nullptr; // capture origin of the loop body
     cudaEvent_t fork    = nullptr;
-    int *loop_counter   = nullptr; // device counter of the loop's passes
-    static constexpr int kChunk = 64; // iterations per pass of the loop body
     struct Graph {
         cudaGraphExec_t exec = nullptr;
-        std::vector<long long> pro, chunk, rest; // kernel launches per member of each piece
-        long passes = 0;
-        int rem     = 0;
+        std::vector<long long> nodes; // kernel launches per member
     };
-    std::map<std::tuple<long, std::vector<const void *>>, Graph> graphs;
+    std::map<std::tuple<int, int, std::vector<const void *>>, Graph> graphs;
 
     ~gpe_batch() {
         cudaSetDevice(device);
@@ -1721,78 +1746,29 @@ struct gpe_batch {
             cudaGraphExecDestroy(kv.second.exec);
         for (auto *m : members)
             delete m;
-        if (loop_counter)
-            cudaFree(loop_counter);
         if (fork)
             cudaEventDestroy(fork);
-        if (body)
-            cudaStreamDestroy(body);
         if (root)
             cudaStreamDestroy(root);
         if (own)
             cudaStreamDestroy(own);
     }
 
-    // Every member's piece (kind 20: prologue, 21: `count` iterations) as one
-    // graph branch each, forked from and joined to `origin`.
-    std::vector<long long> branches(int kind, int count, cudaStream_t origin) {
-        std::vector<long long> nodes;
-        GPE_CUDA(cudaEventRecord(fork, origin));
-        for (auto *m : members)
-            nodes.push_back(m->impl->capture_it_branch(kind, count, fork, origin));
-        return nodes;
-    }
-
-    // k imaginary-time iterations of every member as ONE graph launch: the
-    // prologue, a while node whose body runs kChunk iterations of every member
-    // (k / kChunk passes, counted on the device), then the remaining k % kChunk
-    // iterations.
-    void run(long k) {
+    // One launch of the batch graph for (kind, count): kind 20 the IT prologue,
+    // 21 `count` IT iterations of every member.
+    void run(int kind, int count) {
         std::vector<const void *> sig;
         for (auto *m : members)
             sig.push_back(m->impl->psi_ptr());
-        auto key = std::make_tuple(k, sig);
+        auto key = std::make_tuple(kind, count, sig);
         auto it  = graphs.find(key);
         if (it == graphs.end()) {
             Graph g;
-            g.passes = k / kChunk;
-            g.rem    = (int)(k % kChunk);
             GPE_CUDA(cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal));
             try {
-                g.pro = branches(20, 0, root);
-                if (g.passes > 0) {
-                    gpe::k_loop_init<<<1, 1, 0, root>>>(loop_counter, (int)g.passes);
-                    GPE_CUDA(cudaGetLastError());
-                    cudaStreamCaptureStatus st;
-                    cudaGraph_t graph         = nullptr;
-                    const cudaGraphNode_t *dp = nullptr;
-                    size_t nd                 = 0;
-                    GPE_CUDA(cudaStreamGetCaptureInfo(root, &st, nullptr, &graph, &dp, &nd));
-                    cudaGraphConditionalHandle loop;
-                    GPE_CUDA(cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault));
-                    cudaGraphNodeParams cp = {};
-                    cp.type                = cudaGraphNodeTypeConditional;
-                    cp.conditional.handle  = loop;
-                    cp.conditional.type    = cudaGraphCondTypeWhile;
-                    cp.conditional.size    = 1;
-                    cudaGraphNode_t cnode;
-                    GPE_CUDA(cudaGraphAddNode(&cnode, graph, dp, nd, &cp));
-                    GPE_CUDA(cudaStreamUpdateCaptureDependencies(root, &cnode, 1, cudaStreamSetCaptureDependencies));
-                    cudaGraph_t bg = cp.conditional.phGraph_out[0];
-                    GPE_CUDA(cudaStreamBeginCaptureToGraph(body, bg, nullptr, nullptr, 0,
-                                                           cudaStreamCaptureModeThreadLocal));
-                    try {
-                        g.chunk = branches(21, kChunk, body);
-                        gpe::k_loop_step<<<1, 1, 0, body>>>(loop_counter, loop);
-                        GPE_CUDA(cudaGetLastError());
-                    } catch (...) {
-                        cudaStreamEndCapture(body, &bg);
-                        throw;
-                    }
-                    GPE_CUDA(cudaStreamEndCapture(body, &bg));
-                }
-                if (g.rem > 0)
-                    g.rest = branches(21, g.rem, root);
+                GPE_CUDA(cudaEventRecord(fork, root));
+                for (auto *m : members)
+                    g.nodes.push_back(m->impl->capture_it_branch(kind, count, fork, root));
             } catch (...) {
                 cudaGraph_t gr = nullptr;
                 cudaStreamEndCapture(root, &gr);
@@ -1806,15 +1782,9 @@ struct gpe_batch {
             cudaGraphDestroy(gr);
             it = graphs.emplace(key, std::move(g)).first;
         }
-        const Graph &g = it->second;
-        GPE_CUDA(cudaGraphLaunch(g.exec, cur));
-        for (size_t m = 0; m < members.size(); ++m) {
-            members[m]->impl->it_batch_after(20, 0, g.pro[m]);
-            for (long p = 0; p < g.passes; ++p)
-                members[m]->impl->it_batch_after(21, kChunk, g.chunk[m]);
-            if (g.rem > 0)
-                members[m]->impl->it_batch_after(21, g.rem, g.rest[m]);
-        }
+        GPE_CUDA(cudaGraphLaunch(it->second.exec, cur));
+        for (size_t m = 0; m < members.size(); ++m)
+            members[m]->impl->it_batch_after(kind, count, it->second.nodes[m]);
     }
 };
 
@@ -1965,9 +1935,7 @@ int gpe_batch_create(const gpe_params *members, int count, gpe_batch **out) {
         GPE_CUDA(cudaSetDevice(b->device));
         GPE_CUDA(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking));
         GPE_CUDA(cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking));
-        GPE_CUDA(cudaStreamCreateWithFlags(&b->body, cudaStreamNonBlocking));
         GPE_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
-        GPE_CUDA(cudaMalloc(&b->loop_counter, sizeof(int)));
         b->cur = b->own;
         for (int m = 0; m < count; ++m) {
             gpe_handle *h = nullptr;
@@ -2020,9 +1988,17 @@ int gpe_batch_imag_steps(gpe_batch *b, long k) {
     return guarded([&] {
         for (auto *m : b->members)
             m->impl->it_batch_begin();
-        // the fused imaginary-time schedule of every member (fused_imag:
-        // prologue, chunks of 64 iterations, remainder) in one graph launch
-        b->run(k);
+        // the fused imaginary-time schedule of every member (fused_imag):
+        // prologue, chunks of 64 iterations, remainder
+        b->run(20, 0);
+        constexpr int CH = 64;
+        long done        = 0;
+        while (k - done >= CH) {
+            b->run(21, CH);
+            done += CH;
+        }
+        if (k - done > 0)
+            b->run(21, (int)(k - done));
         for (auto *m : b->members)
             m->impl->it_batch_end();
     });
@@ -2084,6 +2060,13 @@ int gpe_export_fi3d(gpe_handle *h, double *fi3d, size_t n) {
     if (!fi3d || n != h->impl->n())
         return bad("gpe_export_fi3d: null pointer or n != nx*ny*nz");
     return guarded([&] { h->impl->export_fi3d(fi3d); });
+}
+
+int gpe_load_fi3d(gpe_handle *h, const double *fi3d, size_t n) {
+    GPE_HANDLE(h);
+    if (!fi3d || n != h->impl->n())
+        return bad("gpe_load_fi3d: null pointer or n != nx*ny*nz");
+    return guarded([&] { h->impl->load_fi3d(fi3d); });
 }
 
 int gpe_calc_fi3d(gpe_handle *h) {

@@ -197,6 +197,14 @@ class B200GrossPitaevskiSolver:
         capi.check(self._L.gpe_export_fi3d(self._h, capi.dptr(out), self.n))
         return out.reshape(self.params.shape)
 
+    def load_fi3d(self, fi3d) -> None:
+        """Sets the dipolar field that the next real-time iteration's first
+        potential half step uses (a resumed run: the checkpoint's field)."""
+        a = np.ascontiguousarray(np.asarray(fi3d, dtype=np.float64).reshape(-1))
+        if a.size != self.n:
+            raise capi.GpeError(capi.GPE_ERR_ARG, "bad fi3d import")
+        capi.check(self._L.gpe_load_fi3d(self._h, capi.dptr(a), self.n))
+
     # -- the pure virtuals (solver.hpp:55-66) -------------------------------
     def calc_fi3d(self) -> None:
         capi.check(self._L.gpe_calc_fi3d(self._h))
@@ -282,7 +290,9 @@ class B200GrossPitaevskiSolver:
         overlaps the next iterations and the file is written in the background.
         resume: {"phase": "imag" | "real", "iteration": it} of a checkpoint whose
         psi has been loaded (load_buffer): the run continues after it, the edd
-        ramp included."""
+        ramp included.  A real-time record with "fi3d_file" (Checkpointer
+        writes one) also restores the dipolar field the next iteration's first
+        half step uses, so the resumed run repeats the uninterrupted one."""
         p = self.params
 
         def at_checkpoint(phase, it):
@@ -331,6 +341,8 @@ class B200GrossPitaevskiSolver:
                 self.load_pote(request_free_potential())
             else:
                 self.init_pote("MEXICAN_FREE")
+        if phase0 == "real" and resume.get("fi3d_file"):
+            self.load_fi3d(np.fromfile(resume["fi3d_file"], dtype=np.float64))
         if p.calc_strategy in ("RT", "FS"):
             real_phase(start)
         if checkpointer is not None:

@@ -128,6 +128,13 @@ int gpe_export_psi_async(gpe_handle *h, double *psi_c128, size_t n);
 int gpe_export_wait(gpe_handle *h);
 /* The dipolar field fi3d as last computed (FP64 copy). */
 int gpe_export_fi3d(gpe_handle *h, double *fi3d, size_t n);
+/* Sets the dipolar field fi3d (n = nx*ny*nz doubles).  The reference keeps fi3d
+ * in its solver state between real-time iterations: real_time_iter
+ * (solver.cpp:107-112) starts with a potential half step that uses the fi3d of
+ * the previous iteration's calc_fi3d, which psi alone does not determine.  A run
+ * resumed from a checkpoint loads psi and this field to continue exactly where
+ * it stopped.  No counterpart in the reference, which has no resume. */
+int gpe_load_fi3d(gpe_handle *h, const double *fi3d, size_t n);
 
 /* --- the pure virtuals of AbstractGrossPitaevskiSolver (solver.hpp:55-66) --- */
 
