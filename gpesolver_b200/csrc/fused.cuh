@@ -69,18 +69,6 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Programmatic dependent launch.  The pipeline kernels are launched with the
-// programmatic stream serialization attribute: each lets the next kernel of its
-// stream be scheduled as soon as all of its own CTAs are running
-// (pdl_launch_dependents), and waits for the previous kernel to complete, its
-// writes visible, only where it first touches that kernel's results (pdl_wait);
-// loads of constant tables go before the wait.  Without the attribute both are
-// no-ops.
-__device__ __forceinline__ void pdl_launch_dependents() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
 
 // ---------------------------------------------------------------------------
 // X pencils
@@ -106,8 +94,6 @@ __global__ void __launch_bounds__(NT)
     using Iv = LinePass<+1, R, NX, CNT, CNT, NT, true, true>;
     static_assert(Fw::RL == Iv::R0 && Fw::ROUNDSL == Iv::ROUNDS0 && Fw::ITEMSL == Iv::ITEMS0,
                   "paired transforms share the register layout");
-    pdl_launch_dependents();
-    pdl_wait();
     const int tid  = threadIdx.x;
     C *buf         = reinterpret_cast<C *>(g_smem);
     const C *tw    = (const C *)tk.tw, *tl = (const C *)tk.lo;
@@ -178,7 +164,6 @@ __global__ void __launch_bounds__(NT, NX >= 256 ? 2 : 3) // 512-point lines: two
     R *vs          = reinterpret_cast<R *>(tws + L);   // V_dd of |kx| = 0..NX, line b: vs[|kx| CNT + b]
     const C *tw    = (const C *)td.tw;
     const C *twu   = TW2 ? tws : tw;                   // the table the stages read
-    pdl_launch_dependents();
     const int cols = 2 * ny * nz;
     const int c0   = blockIdx.x * CNT;
     const int cnt  = min(CNT, cols - c0);
@@ -193,7 +178,6 @@ __global__ void __launch_bounds__(NT, NX >= 256 ? 2 : 3) // 512-point lines: two
         cp_async4(&vs[e], &vk[(size_t)ix * xs + (size_t)iy * nz + kz]);
     }
     cp_async_commit();
-    pdl_wait(); // the spectrum (and, in imaginary time, the divisor) of the previous kernel
     auto ld = [&](int b, int t) { return b < cnt ? S[(size_t)t * cols + c0 + b] : C{(R)0, (R)0}; };
     C a[Fw::ROUNDSL][Fw::RL];
     Fw::stage0_to_tile(buf, ld, tid);

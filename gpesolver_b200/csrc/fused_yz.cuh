@@ -420,9 +420,6 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     C *Pr_g        = reinterpret_cast<C *>(a.psi_r) + (size_t)i * NY * NZ;
     const R cdd    = (R)a.cdd;
 
-    pdl_launch_dependents();
-    pdl_wait(); // every plane read below is the previous kernel's output
-
     // ---- load the planes (cp.async groups: S; psi and V; kept real-space psi) ---
     if (HAS_INV)
         plane_in_async<C, 2 * NY, NZ, PS, NT>(SP, S_g, tid);

@@ -169,9 +169,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairShape<R, NY, NZ>
     const C *kyt = (const C *)tw.ky.tw, *kyl = (const C *)tw.ky.lo;
     const C *kzt = (const C *)tw.kz.tw, *kzl = (const C *)tw.kz.lo;
 
-    pdl_launch_dependents();
-    pdl_wait(); // the spectra and the kept psi are the previous kernels' output
-
     // ---- loads: the column halves of both spectra; V and the kept psi of this
     // CTA's rows (needed from the C2R's last stage on) ----------------------
 #pragma unroll 4
@@ -462,9 +459,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairShape<R, NY, NZ>
     const bool xin   = i >= 1 && i < nx - 1;
     const C *dyt = (const C *)tw.dy.tw, *dyl = (const C *)tw.dy.lo;
     const C *dzt = (const C *)tw.dz.tw, *dzl = (const C *)tw.dz.lo;
-
-    pdl_launch_dependents();
-    pdl_wait(); // the spectrum, psi and the divisor are the previous kernels' output
 
     // ---- loads: the dipolar column half; V, the psi rows of the stencil ------
 #pragma unroll 4

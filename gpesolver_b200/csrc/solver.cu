@@ -268,8 +268,6 @@ template <class R> class Solver final : public SolverBase {
         GPE_CUDA(cudaStreamSynchronize(cur));
         set_smem_attrs();
         if (fused) {
-            if (const char *e = std::getenv("GPE_PDL"))
-                pdl = e[0] != '0';
             set_fused_attrs();
             autotune_x();
         }
@@ -877,12 +875,12 @@ template <class R> class Solver final : public SolverBase {
     }
     template <int NN, int CNT> void launch_xk(cudaStream_t s) {
         constexpr int NT = pass_threads<NN, CNT>();
-        launch_pdl(k3_x_kin<R, NN, CNT, NT>, (ny * nz + CNT - 1) / CNT, NT, xy_smem<R, NN, CNT>(), s, psi.p,
+        launch(k3_x_kin<R, NN, CNT, NT>, (ny * nz + CNT - 1) / CNT, NT, xy_smem<R, NN, CNT>(), s, psi.p,
                (const C *)ex.p, (const C *)ey.p, (const C *)ez.p, inv_hi, inv_lo, ny, nz, twid(kx));
     }
     template <int NN, int CNT> void launch_xd(cudaStream_t s, const double *divisor, double dscale) {
         constexpr int NT = pass_threads<2 * NN, CNT>();
-        launch_pdl(k3_x_dip<R, NN, CNT, NT>, (2 * ny * nz + CNT - 1) / CNT, NT, x_dip_smem<R, NN, CNT>(), s, S2.p,
+        launch(k3_x_dip<R, NN, CNT, NT>, (2 * ny * nz + CNT - 1) / CNT, NT, x_dip_smem<R, NN, CNT>(), s, S2.p,
                (const R *)vk2.p, divisor, dscale, ny, nz, twid(dx));
     }
     template <int NN> void f_x_n(cudaStream_t s, bool kin, const double *divisor, int part, double dscale) {
@@ -1048,6 +1046,14 @@ template <class R> class Solver final : public SolverBase {
             // the pair replaces the one-CTA kernel only when 3% faster
             pair_rt = trt[1] < 0.97f * trt[0];
             pair_it = tit[1] < 0.97f * tit[0];
+            // The imaginary-time launches divide by the zero norm they leave
+            // behind, so the fields they wrote hold NaN: clear every field the
+            // tuning touched, the norm state and the status, as at creation.
+            GPE_CUDA(cudaMemsetAsync(psi.p, 0, sizeof(C) * N, cur));
+            GPE_CUDA(cudaMemsetAsync(psii.p, 0, sizeof(C) * N, cur));
+            GPE_CUDA(cudaMemsetAsync(psir.p, 0, sizeof(C) * N, cur));
+            GPE_CUDA(cudaMemsetAsync(S2.p, 0, sizeof(C) * S2.n, cur));
+            GPE_CUDA(cudaMemsetAsync(phi.p, 0, sizeof(R) * N, cur));
             GPE_CUDA(cudaMemsetAsync(status.p, 0, sizeof(int) * 4, cur));
             GPE_CUDA(cudaMemcpyAsync(norm_state.p, one_buf.p, sizeof(double), cudaMemcpyDeviceToDevice, cur));
             set_divisor_one();
@@ -1147,13 +1153,13 @@ template <class R> class Solver final : public SolverBase {
     if (ny == A && nz == B) {                                                                      \
         using G = YZShape<R, A, B>;                                                                \
         if (MODE == ZM_RT_MID && pair_rt)                                                          \
-            launch_pdl(k5_yz_pair<R, A, B>, 2 * nx, PairShape<R, A, B>::NT,                        \
-                       PairShape<R, A, B>::SMEM, s, a, t);                                         \
+            launch(k5_yz_pair<R, A, B>, 2 * nx, PairShape<R, A, B>::NT, PairShape<R, A, B>::SMEM,  \
+                   s, a, t);                                                                       \
         else if (MODE == ZM_IT_MID && pair_it)                                                     \
-            launch_pdl(k5_yz_pair_it<R, A, B>, 2 * nx, PairShape<R, A, B>::NT,                     \
-                       PairShapeIT<R, A, B>::SMEM, s, a, t);                                       \
+            launch(k5_yz_pair_it<R, A, B>, 2 * nx, PairShape<R, A, B>::NT,                         \
+                   PairShapeIT<R, A, B>::SMEM, s, a, t);                                           \
         else                                                                                       \
-            launch_pdl(k4_yz<R, A, B, MODE>, nx, G::NT, G::template smem<MODE>(), s, a, t);       \
+            launch(k4_yz<R, A, B, MODE>, nx, G::NT, G::template smem<MODE>(), s, a, t);           \
     }
             GPE_YZ_CASES(GPE_LYZ)
 #undef GPE_LYZ
@@ -1230,10 +1236,8 @@ template <class R> class Solver final : public SolverBase {
                     break;
                 GPE_CUDA(cudaEventRecord(ev_fork, s));
                 GPE_CUDA(cudaStreamWaitEvent(s2, ev_fork, 0));
-                // the dipolar pencils (the longer branch) follow the plane kernel
-                // on its own stream, the kinetic ones run beside them
-                f_x(s, false, nullptr);
-                f_x(s2, true, nullptr, 1);
+                f_x(s, true, nullptr, 1);
+                f_x(s2, false, nullptr);
                 GPE_CUDA(cudaEventRecord(ev_join, s2));
                 GPE_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
                 if (t == count) {
@@ -1335,7 +1339,6 @@ template <class R> class Solver final : public SolverBase {
     // middle real- / imaginary-time iterations on the two-CTA plane kernels
     // (k5_yz_pair, k5_yz_pair_it) instead of k4_yz: picked by autotune_x
     bool pair_rt = false, pair_it = false;
-    bool pdl     = true; // programmatic dependent launch of the pipeline kernels (GPE_PDL=0: off)
     DevBuf<C> S2;
     DevBuf<C> psir; // real time: psi in real space after the last phase step
     int xk_lines = 16, xd_lines = 16; // x-pass lines per CTA (autotune_x)
@@ -1368,29 +1371,6 @@ template <class R> class Solver final : public SolverBase {
     void launch(K kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
         kernel<<<grid, block, smem, s>>>(args...);
         GPE_CUDA(cudaGetLastError());
-        ++n_launch;
-    }
-    // A pipeline kernel launched with programmatic stream serialization: it may
-    // be scheduled while the previous kernel of its stream finishes, and waits
-    // for that kernel's results inside (pdl_wait).  GPE_PDL=0 launches plainly.
-    template <class... KArgs, class... Args>
-    void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                    Args... args) {
-        if (!pdl) {
-            launch(kernel, grid, block, smem, s, args...);
-            return;
-        }
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim            = grid;
-        cfg.blockDim           = block;
-        cfg.dynamicSmemBytes   = smem;
-        cfg.stream             = s;
-        cudaLaunchAttribute at[1];
-        at[0].id                                         = cudaLaunchAttributeProgrammaticStreamSerialization;
-        at[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs                                        = at;
-        cfg.numAttrs                                     = 1;
-        GPE_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
         ++n_launch;
     }
 

@@ -82,3 +82,40 @@ def test_plane_pair_kernel_matches_one_cta_plane_kernel(dims, monkeypatch):
     assert rel_l2(a[0], b[0]) < 1e-6 and rel_l2(a[1], b[1]) < 1e-6
     assert abs(a[2] - b[2]) < 1e-12 * abs(b[2])
     assert rel_l2(a[3], b[3]) < 1e-6 and rel_l2(a[4], b[4]) < 1e-6
+
+
+@pytest.mark.gpu
+def test_first_solver_of_a_grid_is_clean_after_tuning():
+    """The first solver of a grid on a device runs the autotuner, whose
+    imaginary-time candidates leave a zero norm (and NaN behind it) in the
+    fields they wrote; the solver must come out as if just created: a finite
+    energy before any iteration, and the same iterations as a solver that
+    reused the tuner's choice.  Run in a fresh process so that no earlier test
+    has tuned the grid."""
+    import os
+    import subprocess
+    import sys
+
+    code = """
+import numpy as np, sys
+sys.path.insert(0, %r)
+import gpesolver_b200 as G
+from tests.helpers import WELL_CONDITIONED, gparams
+p = gparams(WELL_CONDITIONED(64, 64, 16))
+out = []
+for _ in range(2):  # the first solver tunes, the second reuses the choice
+    with G.B200GrossPitaevskiSolver(p, precision="c64") as s:
+        s.init_pote()
+        s.init_buffer()
+        e0 = s.calc_energy().e_total
+        assert np.isfinite(e0), e0
+        s.imag_steps(30)
+        s.real_steps(30, 0)
+        out.append(s.export_data().copy())
+d = np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[1])
+assert d == 0.0, d
+print("ok")
+""" % os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("GPE_PLANE_PAIR", "GPE_X_TILES", "GPE_Y_LINES")}
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
