@@ -110,6 +110,30 @@ struct PlanePass {
             }
         }
 
+        // stage-0 butterfly inputs straight from a loader ld(b, t) (element t of
+        // line b), for a first stage that reads global memory instead of the
+        // tile (no twiddles: the first stage has none)
+        template <class Ld> static __device__ __forceinline__ void read_ld(Ld &ld, Regs &a, int tid) {
+            static_assert(S == 0, "only the first stage reads through a loader");
+#pragma unroll
+            for (int rd = 0; rd < ROUNDS; ++rd) {
+                const int it = rd * NT + tid;
+                if (!valid(it))
+                    break;
+                const int j = it / COUNT;
+                const int b = it - j * COUNT;
+#pragma unroll
+                for (int k = 0; k < RADIX; ++k)
+                    a[rd][k] = (PIN && 2 * k >= RADIX) ? C{(R)0, (R)0} : ld(b, j + k * NR);
+            }
+#pragma unroll
+            for (int rd = 0; rd < ROUNDS; ++rd) {
+                if (!valid(rd * NT + tid))
+                    break;
+                DFTZ<RADIX, SIGN, R, CMP, PIN ? RADIX / 2 : RADIX>::run(a[rd]);
+            }
+        }
+
         static __device__ __forceinline__ void write(C *buf, const Regs &a, int tid) {
 #pragma unroll
             for (int rd = 0; rd < ROUNDS; ++rd) {
@@ -325,11 +349,20 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
     // phi (FP holds V on entry), and phi -> global when WRITE_PHI.  SP must be
     // loaded (caller synchronised); the caller's other cp.async group (psi, V)
     // is waited for here, overlapped with the y transforms.
+    // S_g: the plane of the spectrum in global memory, read by the first stage
+    // of the y transform (which writes SP)
     template <bool WRITE_PHI>
-    static __device__ __forceinline__ void inverse(C *SP, C *DP, R *FP, R *phi_g, R cdd, const YZTwid &tw,
-                                                   int t) {
-        PlanePass<+1, R, 2 * NY, NZ, 1, PS, NTG, false, true, false, true, BAR>::run(
-            SP, (const C *)tw.dy.tw, (const C *)tw.dy.lo, t);
+    static __device__ __forceinline__ void inverse(const C *S_g, C *SP, C *DP, R *FP, R *phi_g, R cdd,
+                                                   const YZTwid &tw, int t) {
+        using DYI = PlanePass<+1, R, 2 * NY, NZ, 1, PS, NTG, false, true, false, true, BAR>;
+        {
+            auto lds = [&](int b, int r) { return S_g[r * NZ + b]; };
+            typename DYI::First::Regs a0;
+            DYI::First::read_ld(lds, a0, t);
+            DYI::First::write(SP, a0, t);
+            group_sync<BAR, NTG>();
+        }
+        DYI::template stages<1, DYI::NSTG>(SP, (const C *)tw.dy.tw, (const C *)tw.dy.lo, t);
         cp_async_wait<0>(); // visible to the block after the next barrier
         // pair lines: z[m] = X_a[m] + i X_b[m] over the full 2nz-point spectrum
         // (bins 1..nz stored at kz - 1, bin 0 is zero, bins > nz by symmetry);
@@ -420,11 +453,16 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     C *Pr_g        = reinterpret_cast<C *>(a.psi_r) + (size_t)i * NY * NZ;
     const R cdd    = (R)a.cdd;
 
-    // ---- load the planes (cp.async groups: S; psi and V; kept real-space psi) ---
-    if (HAS_INV)
-        plane_in_async<C, 2 * NY, NZ, PS, NT>(SP, S_g, tid);
+    // ---- load the planes (cp.async groups: none; psi and V; kept real-space psi) ---
+    // In real time with the inverse transforms (middle and last iterations) the
+    // first stages of the inverse y transforms read the S and psi planes from
+    // global memory themselves (RT_DIRECT below): the tile is written once, by
+    // those stages, instead of by the copy and again by them.
+    // (In imaginary time the dipolar inverse's first stage reads the S plane
+    // from global memory the same way.)
+    constexpr bool RT_DIRECT = RT && HAS_INV;
     cp_async_commit();
-    if (RT || MODE == ZM_IT_MID)
+    if ((RT || MODE == ZM_IT_MID) && !RT_DIRECT)
         plane_in_async<C, NY, NZ, PS, NT>(PP, reinterpret_cast<const C *>(a.psi_in) + (size_t)i * NY * NZ, tid);
     if (MODE != ZM_IT_PRO) {
 #pragma unroll 4
@@ -441,10 +479,10 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     cp_async_commit();
     constexpr bool KEPT = MODE == ZM_RT_MID || MODE == ZM_RT_EPI;
     if (KEPT) {
-        // needed only at the phase step: waited for there, behind the transforms
+        // needed only at the phase step: waited for there, behind the transforms;
+        // V (the group before) is waited for before the C2R's stages
         plane_in_async<C, NY, NZ, PS, NT>(RP, Pr_g, tid);
         cp_async_commit();
-        cp_async_wait<1>();
     } else if (HAS_INV && !RT) {
         cp_async_wait<1>(); // S; psi and V are waited for inside the dipolar inverse
     } else {
@@ -475,8 +513,22 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
         constexpr bool WRITE_PHI = MODE != ZM_RT_MID; // read only after the last iteration
         typename ZI::Last::Regs zr;
         if (HAS_INV) {
-            // dipolar iFFT_y (lower half kept) || kinetic iFFT_y
-            joint_stages<DYI, 0, DYI::NSTG, KYI, 0, KYI::NSTG>(SP, dyt, dyl, PP, kyt, kyl, tid);
+            // dipolar iFFT_y (lower half kept) || kinetic iFFT_y; their first
+            // stages load the planes from global memory (coalesced along the
+            // nz columns) and write the tiles
+            {
+                const C *Q_g = reinterpret_cast<const C *>(a.psi_in) + (size_t)i * NY * NZ;
+                auto lds     = [&](int b, int t) { return S_g[t * NZ + b]; };
+                auto ldq     = [&](int b, int t) { return Q_g[t * NZ + b]; };
+                typename DYI::First::Regs da0;
+                typename KYI::First::Regs ka0;
+                DYI::First::read_ld(lds, da0, tid);
+                KYI::First::read_ld(ldq, ka0, tid);
+                DYI::First::write(SP, da0, tid);
+                KYI::First::write(PP, ka0, tid);
+                __syncthreads();
+            }
+            joint_stages<DYI, 1, DYI::NSTG, KYI, 1, KYI::NSTG>(SP, dyt, dyl, PP, kyt, kyl, tid);
             // C2R pair lines: z[m] = X_a[m] + i X_b[m] over the full 2nz-point
             // spectrum (bins 1..nz stored at kz - 1, bin 0 zero, bins > nz by
             // symmetry); DP shares SP's upper half, which holds nothing now;
@@ -497,6 +549,8 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                 }
                 DP[p + m * TD] = z;
             }
+            if (KEPT)
+                cp_async_wait<1>(); // V: visible to the block after the barriers below
             __syncthreads();
             // C2R || kinetic iFFT_z, all stages but the last
             joint_stages<C2R, 0, C2R::NSTG - 1, ZI, 0, ZI::NSTG - 1>(DP, dzt, dzl, PP, kzt, kzl, tid);
@@ -691,7 +745,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                 FP[G::fpi(r, k)] = wat * (p.x * p.x + p.y * p.y);
             }
         } else {
-            DW::template inverse<true>(SP, DP, FP, phi_g, cdd, tw, tid);
+            DW::template inverse<true>(S_g, SP, DP, FP, phi_g, cdd, tw, tid);
             __syncthreads(); // FP complete
             const StepCoef cf = a.step.coef[0];
             const R g3w = (R)cf.g3w, gw15 = (R)cf.gw15;

@@ -13,9 +13,10 @@ pytestmark = pytest.mark.gpu
 CHOICES = {(8, 8), (8, 16), (16, 8), (16, 16)}
 
 
-@pytest.mark.parametrize("dims", [(64, 64, 16), (32, 256, 16)])
+@pytest.mark.parametrize("dims", [(64, 64, 16), (96, 96, 24), (32, 256, 16)])
 def test_x_tile_choices_give_identical_results(dims, monkeypatch):
-    # the plane-kernel schedule (64^2 x 16) and the four-kernel one (32 x 256 x 16)
+    # the plane-kernel schedule (64^2 x 16; 96^2 x 24, whose x lines take three
+    # stages) and the four-kernel one (32 x 256 x 16)
     p = gparams(WELL_CONDITIONED(*dims))
     V, psi0 = G.potential(p), G.initial_psi(p)
     outs = []
@@ -29,7 +30,12 @@ def test_x_tile_choices_give_identical_results(dims, monkeypatch):
             s.real_steps(20, 0)
             outs.append(s.export_data())
     for o in outs[1:]:
-        np.testing.assert_array_equal(o, outs[0])
+        if dims[0] == 96:
+            # lines of 3 x 8 x 8 points: the widths' instances agree to FP32
+            # rounding, not to the bit (measured: 7e-15 absolute on |psi| ~1e-6)
+            assert rel_l2(o, outs[0]) < 1e-6
+        else:
+            np.testing.assert_array_equal(o, outs[0])
 
 
 def test_autotuner_choice_is_reused_per_grid(monkeypatch):
@@ -68,6 +74,7 @@ def test_plane_pair_kernel_matches_one_cta_plane_kernel(dims, monkeypatch):
     planes), so psi and phi agree to rounding (1e-6)."""
     p = gparams(WELL_CONDITIONED(*dims))
     out = {}
+    monkeypatch.setenv("GPE_X_TILES", "16,16")  # the same x pass in both runs
     for pair in ("1", "0"):
         monkeypatch.setenv("GPE_PLANE_PAIR", pair)
         with G.B200GrossPitaevskiSolver(p, precision="c64") as s:

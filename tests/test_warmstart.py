@@ -76,3 +76,35 @@ def test_trained_network_shortens_imaginary_time():
     # in fewer iterations
     assert same >= len(held_p) // 2, same
     assert np.median(gain) > 1.2, gain
+
+
+def test_committed_network_shortens_imaginary_time_at_128():
+    """The committed 128x128x32 network (gpesolver_b200/data) on the first 8
+    held-out solves of the warm-start study (SplitMix64 seed 2000, CYLINDRICAL,
+    edd, n_atoms, omega_r, omega_z / omega_r over the sweep ranges): imaginary
+    time from its prediction and from the Gaussian start both run to dE/E <
+    1e-8 between checks 10 iterations apart.  On a B200 the warm starts took
+    2.0-4.1x fewer iterations (median 3.1x) and all reached the Gaussian start's
+    state; over all 32 held-out solves the median time ratio was 2.35x (29 of
+    32 in the same state), short of the 3x target.  Held here: the same state
+    for at least 7 of 8, a median iteration ratio of at least 2.5, none below
+    1.5."""
+    grids = ((128, 128, 32),)
+    held_p = sweep.sweep_params(count=8, seed=2000, grids=grids)
+    net = W.WarmStartNet.pretrained()
+    ratios, same = [], 0
+    for p in held_p:
+        with G.B200GrossPitaevskiSolver(p) as a, G.B200GrossPitaevskiSolver(p) as b:
+            for s in (a, b):
+                s.init_pote()
+            a.init_buffer("GAUSS")
+            net.predict_into(b)
+            ia, _, ea = W.time_to_ground_state(a)
+            ib, _, eb = W.time_to_ground_state(b)
+            if abs(ea - eb) <= 1e-5 * abs(ea):
+                same += 1
+                ratios.append(ia / ib)
+    net.close()
+    assert same >= 7, same
+    assert np.median(ratios) >= 2.5, ratios
+    assert min(ratios) >= 1.5, ratios
