@@ -69,6 +69,45 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// One-dimensional bulk copies (global -> this CTA's shared memory) completing
+// on an mbarrier: one thread arms the barrier with the byte count and issues
+// the copies, every thread waits for the barrier's phase.  Addresses and sizes
+// must be multiples of 16 bytes.  No multicast: each CTA copies into its own
+// shared memory.
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+    // make the initialised barrier visible to the async proxy (the bulk copies)
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *smem, const void *g, unsigned bytes, unsigned long long *bar) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(s),
+                 "l"(g), "r"(bytes), "r"(b)
+                 : "memory");
+}
+// Waits for phase `parity` of the barrier, at most `tries` polls (each poll may
+// suspend the thread for a while); false when it gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int tries) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    for (int t = 0; t < tries; ++t) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(a), "r"(parity)
+                     : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+
 
 // ---------------------------------------------------------------------------
 // X pencils

@@ -29,6 +29,10 @@
 //   RP   ny rows x PS  real-space psi of the previous phase step (real time,
 //       middle and last iterations)
 //   XM, XP  ny rows x PS each: psi of planes i - 1 and i + 1 (imaginary time)
+// In the middle imaginary-time iterations PP, XM and XP hold the three psi
+// planes of the stencil unpadded (ny rows x nz: the stencil reads them row by
+// row, consecutive threads on consecutive z), each brought in by one 1-D bulk
+// copy of the contiguous plane that completes on an mbarrier.
 #pragma once
 
 #include "fused.cuh"
@@ -461,8 +465,10 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
     // (In imaginary time the dipolar inverse's first stage reads the S plane
     // from global memory the same way.)
     constexpr bool RT_DIRECT = RT && HAS_INV;
+    constexpr bool IT_BULK   = MODE == ZM_IT_MID; // the stencil's planes by bulk copies
+    __shared__ __align__(8) unsigned long long pbar;
     cp_async_commit();
-    if ((RT || MODE == ZM_IT_MID) && !RT_DIRECT)
+    if (RT && !RT_DIRECT)
         plane_in_async<C, NY, NZ, PS, NT>(PP, reinterpret_cast<const C *>(a.psi_in) + (size_t)i * NY * NZ, tid);
     if (MODE != ZM_IT_PRO) {
 #pragma unroll 4
@@ -471,10 +477,19 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
             cp_async4(&FP[G::fpi(r, k)], &V_g[e]);
         }
     }
-    if (MODE == ZM_IT_MID && i >= 1 && i < nx - 1) {
-        const C *pin = reinterpret_cast<const C *>(a.psi_in);
-        plane_in_async<C, NY, NZ, PS, NT>(XM, pin + (size_t)(i - 1) * NY * NZ, tid);
-        plane_in_async<C, NY, NZ, PS, NT>(XP, pin + (size_t)(i + 1) * NY * NZ, tid);
+    if (IT_BULK && tid == 0) {
+        // psi of this plane and (interior planes) of its two x neighbours:
+        // three contiguous 8 ny nz-byte blocks, one bulk copy each
+        const C *pin      = reinterpret_cast<const C *>(a.psi_in);
+        const bool inner  = i >= 1 && i < nx - 1;
+        const unsigned pb = (unsigned)(sizeof(C) * NY * NZ);
+        mbar_init(&pbar, 1);
+        mbar_expect_tx(&pbar, inner ? 3 * pb : pb);
+        bulk_g2s(PP, pin + (size_t)i * NY * NZ, pb, &pbar);
+        if (inner) {
+            bulk_g2s(XM, pin + (size_t)(i - 1) * NY * NZ, pb, &pbar);
+            bulk_g2s(XP, pin + (size_t)(i + 1) * NY * NZ, pb, &pbar);
+        }
     }
     cp_async_commit();
     constexpr bool KEPT = MODE == ZM_RT_MID || MODE == ZM_RT_EPI;
@@ -751,6 +766,12 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
             const R g3w = (R)cf.g3w, gw15 = (R)cf.gw15;
             const R cx = (R)a.cx, cy = (R)a.cy, cz = (R)a.cz, dtau = (R)a.dtau;
             const bool xin = i >= 1 && i < nx - 1;
+            // the three planes (bulk copies issued at kernel start); a copy that
+            // has not landed after the bounded wait is reported in status[1]
+            if (!mbar_wait(&pbar, 0, 1 << 22)) {
+                a.status[1] = 1;
+                mbar_wait(&pbar, 0, 1 << 22);
+            }
 #pragma unroll 2
             for (int e = tid; e < NY * NZ; e += NT) {
                 const int r = e / NZ, k = e - r * NZ;
@@ -759,10 +780,10 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid 
                 if (!xin || r < 1 || r >= NY - 1 || k < 1 || k >= NZ - 1) {
                     o = __ldg(&bnd[q]);
                 } else {
-                    const C *pp = PP + r * PS + k; // this plane and its x neighbours (shared)
+                    const C *pp = PP + e; // this plane and its x neighbours (unpadded)
                     const C c0 = cscale(pp[0], sc);
-                    const C xm = cscale(XM[r * PS + k], sc), xp = cscale(XP[r * PS + k], sc);
-                    const C ym = cscale(pp[-PS], sc), yp = cscale(pp[PS], sc);
+                    const C xm = cscale(XM[e], sc), xp = cscale(XP[e], sc);
+                    const C ym = cscale(pp[-NZ], sc), yp = cscale(pp[NZ], sc);
                     const C zm = cscale(pp[-1], sc), zp = cscale(pp[1], sc);
                     const R vv   = FP[G::fpi(r, k)];
                     const R dens = c0.x * c0.x + c0.y * c0.y;

@@ -1487,12 +1487,16 @@ template <class R> class Solver final : public SolverBase {
         lazy = false;
     }
 
+    // status[0]: a non-finite or non-positive norm; status[1]: a bulk copy into
+    // shared memory that a plane kernel stopped waiting for
     void check_status() {
-        int st = 0;
-        GPE_CUDA(cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, cur));
+        int st[2] = {0, 0};
+        GPE_CUDA(cudaMemcpyAsync(st, status.p, sizeof(st), cudaMemcpyDeviceToHost, cur));
         GPE_CUDA(cudaStreamSynchronize(cur));
-        if (st != 0) {
-            GPE_CUDA(cudaMemset(status.p, 0, sizeof(int)));
+        if (st[0] != 0 || st[1] != 0) {
+            GPE_CUDA(cudaMemset(status.p, 0, sizeof(st)));
+            if (st[1] != 0)
+                throw Error(GPE_ERR_CUDA, "a plane kernel's bulk copy into shared memory did not complete");
             throw Error(GPE_ERR_NUMERIC, "non-finite or non-positive norm of psi");
         }
     }
