@@ -341,6 +341,12 @@ template <class R, int NY, int NZ> struct YZShape {
     }
     static constexpr int NT0     = 2 * NY * NZ / 16;
     static constexpr int NT      = NT0 < 128 ? 128 : (NT0 > 512 ? 512 : (NT0 + 31) / 32 * 32);
+    // Threads of the kernel in each mode: the imaginary-time modes (62-80
+    // registers, no kinetic chain; latency bound on their plane loads) run twice
+    // the real-time count, at most 1024.
+    template <int MODE> static constexpr int nt() {
+        return (MODE == ZM_IT_PRO || MODE == ZM_IT_MID) ? (2 * NT > 1024 ? 1024 : 2 * NT) : NT;
+    }
 };
 
 // The dipolar chain of a plane, run by NTG threads of barrier group BAR.
@@ -430,10 +436,10 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
 };
 
 template <class R, int NY, int NZ, int MODE>
-__global__ void __launch_bounds__(YZShape<R, NY, NZ>::NT) k4_yz(ZArgs a, YZTwid tw) {
+__global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz(ZArgs a, YZTwid tw) {
     using C                = cplx<R>;
     using G                = YZShape<R, NY, NZ>;
-    constexpr int NT       = G::NT;
+    constexpr int NT       = G::template nt<MODE>();
     constexpr int PS       = G::PS;
     constexpr bool RT      = MODE <= ZM_RT_EPI;
     constexpr bool HAS_INV = (MODE == ZM_RT_MID || MODE == ZM_RT_EPI || MODE == ZM_IT_MID);

@@ -1159,7 +1159,7 @@ template <class R> class Solver final : public SolverBase {
             launch(k5_yz_pair_it<R, A, B>, 2 * nx, PairShape<R, A, B>::NT,                         \
                    PairShapeIT<R, A, B>::SMEM, s, a, t);                                           \
         else                                                                                       \
-            launch(k4_yz<R, A, B, MODE>, nx, G::NT, G::template smem<MODE>(), s, a, t);           \
+            launch(k4_yz<R, A, B, MODE>, nx, G::template nt<MODE>(), G::template smem<MODE>(), s, a, t); \
     }
             GPE_YZ_CASES(GPE_LYZ)
 #undef GPE_LYZ
