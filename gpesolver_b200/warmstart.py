@@ -6,7 +6,8 @@ predicts the ground-state amplitude |psi_0| on the solver grid, and
 ``predict_into`` loads that amplitude into a solver as its initial state
 (load_buffer semantics, without a host round trip).  Imaginary time then
 refines it to the same energy tolerance as a Gaussian start; plain
-Gaussian-start imaginary time remains the fallback and the judge.
+Gaussian-start imaginary time remains the fallback and the yardstick for the
+prediction's error.
 
 The training data are ground states that the plain method produces
 (``ground_states``, batched with B200Batch); ``train`` runs Adam on them with
