@@ -805,7 +805,9 @@ def run_sweep(args):
                                f"omega_z/omega_r~U[1,4], dx=dy=120 nm, dz=600 nm",
                    "grids": {f"{g[0]}x{g[1]}x{g[2]}": c for g, c in sorted(counts.items())},
                    "seed": 0, "generator": "SplitMix64",
-                   "schedule": "one CUDA graph per 64-iteration chunk, one branch per member",
+                   "schedule": (f"one CUDA graph launch for the {iters} iterations, one independent branch "
+                                "per member" if iters <= 1024 else
+                                "one CUDA graph launch per 1024 iterations, one branch per member"),
                    "l2": "flushed before each timed sweep"},
         "sweep_seconds": t,
         "sequential_gpu": ({"value": len(ps) * iters / seq, "sweep_seconds": seq,

@@ -3,8 +3,9 @@
 A parameter sweep (trap, atom number, dipolar strength, grid) is a set of
 independent imaginary-time solves.  ``B200Batch`` creates them as one
 ``gpe_batch`` (include/gpe_b200.h): every member's fused iteration chain is a
-branch of the same CUDA graph, so one graph launch per chunk of iterations runs
-all members side by side and small grids fill the GPU together.  Each member
+branch of the same CUDA graph, so one graph launch (per call of up to 1024
+iterations) runs all members side by side and small grids fill the GPU
+together.  Each member
 is a ``B200GrossPitaevskiSolver`` view for loading, device-side initialisation,
 export and energies; the reference runs each member as a separate process.
 """

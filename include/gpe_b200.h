@@ -242,8 +242,10 @@ int gpe_export_potential(gpe_handle *h, double *V, size_t n);
 /* --- batched imaginary time (parameter sweeps) --- */
 
 /* A set of independent solves on one GPU whose imaginary-time iterations run
- * as one CUDA-graph launch per chunk of iterations: every member's kernel chain
- * is a branch of the same graph, so small grids fill the GPU together.  The
+ * as one CUDA-graph launch per call of up to 1024 iterations (longer calls: one
+ * launch per 1024; GPE_BATCH_CHUNK=1..4096 sets the count): every member's
+ * kernel chain is an independent branch of the same graph, joined only at its
+ * end, so small grids fill the GPU together.  The
  * reference runs such sweeps as separate processes, one after the other.
  * Members may differ in grid and parameters; each must take the fused
  * complex64 pipeline (compiled grid sizes). */
