@@ -51,9 +51,11 @@ template <int BAR, int NTG> __device__ __forceinline__ void group_sync() {
 // All stages of a transform over a tile in shared memory, in place (each stage
 // reads its butterflies into registers, synchronises, writes, synchronises).
 // Element t of line b at buf[b*BS + t*TS].  NT threads of barrier group BAR
-// take part (tid = index within the group).
+// take part (tid = index within the group).  TWS: the twiddle tables passed
+// to the stages are in shared memory (plain loads instead of read-only global
+// loads).
 template <int SIGN, class R, int L, int COUNT, int BS, int TS, int NT, bool CMP, bool REV, bool IH = false,
-          bool OH = false, int BAR = 0>
+          bool OH = false, int BAR = 0, bool TWS = false>
 struct PlanePass {
     using C                      = cplx<R>;
     static constexpr Radices RAD = REV ? reversed(radices_of(L)) : radices_of(L);
@@ -102,9 +104,9 @@ struct PlanePass {
                     C v = s[k * NR * TS];
                     if (NS > 1 && k > 0) {
                         const int t = jm * k * STEP;
-                        const C w   = __ldg(&tw[t]);
+                        const C w   = TWS ? tw[t] : __ldg(&tw[t]);
                         if constexpr (sizeof(R) == 4 && CMP)
-                            v = twmul<SIGN>(v, w, __ldg(&twlo[t]));
+                            v = twmul<SIGN>(v, w, TWS ? twlo[t] : __ldg(&twlo[t]));
                         else
                             v = SIGN < 0 ? cmul(v, w) : cmulc(v, w);
                     }
@@ -186,9 +188,9 @@ struct PlanePass {
     // All stages, the last one handing its outputs to st(b, t, v) (element t of
     // line b) instead of writing the tile.  Other threads may still read the
     // tile on return: synchronise before reusing it.
-    template <class St>
+    template <int S0 = 0, class St>
     static __device__ __forceinline__ void run_emit(C *buf, St st, const C *tw, const C *twlo, int tid) {
-        stages<0, NSTG - 1>(buf, tw, twlo, tid);
+        stages<S0, NSTG - 1>(buf, tw, twlo, tid);
         typename Last::Regs a;
         Last::read(buf, a, tw, twlo, tid);
 #pragma unroll
@@ -336,8 +338,43 @@ template <class R, int NY, int NZ> struct YZShape {
     static constexpr size_t RP_B = sizeof(C) * NY * PS;
     static constexpr size_t SMEM_RT = SMEM + RP_B;            // RT middle and last iterations
     static constexpr size_t SMEM_IT = SMEM + 2 * RP_B;        // IT: the two x-neighbour planes
-    template <int MODE> static constexpr size_t smem() {
+    template <int MODE> static constexpr size_t smem_base() {
         return (MODE == ZM_RT_MID || MODE == ZM_RT_EPI) ? SMEM_RT : (MODE == ZM_IT_MID ? SMEM_IT : SMEM);
+    }
+    // The twiddle tables, staged in shared memory behind the tiles (TW): the
+    // dipolar y (2ny) and z (2nz) lines, the kinetic y (ny) and z (nz) lines
+    // with their rounding remainders.  One SM runs one plane per launch, so its
+    // L1 holds none of them at kernel start: read from global memory, every
+    // stage's first twiddle loads would wait for L2.
+    static constexpr int TW_DY = 0, TW_DZ = 2 * NY, TW_KY = TW_DZ + LD, TW_KYL = TW_KY + NY,
+                         TW_KZ = TW_KYL + NY, TW_KZL = TW_KZ + NZ, TWN = TW_KZL + NZ;
+    static constexpr size_t TW_B = sizeof(C) * TWN;
+    static_assert(SMEM % 8 == 0 && SMEM_RT % 8 == 0 && SMEM_IT % 8 == 0, "8-byte aligned twiddle region");
+    template <int MODE> static constexpr size_t smem() {
+        return smem_base<MODE>() + (MODE <= ZM_RT_EPI ? TW_B : 0);
+    }
+    // cp.async of the tables into TW (real time)
+    static __device__ __forceinline__ void twiddles_in(C *TW, const YZTwid &tw, int tid, int nt) {
+        auto cp = [&](int off, const void *src, int n) {
+            for (int e = tid; e < n; e += nt)
+                cp_async8(&TW[off + e], reinterpret_cast<const C *>(src) + e);
+        };
+        cp(TW_DY, tw.dy.tw, 2 * NY);
+        cp(TW_DZ, tw.dz.tw, LD);
+        cp(TW_KY, tw.ky.tw, NY);
+        cp(TW_KYL, tw.ky.lo, NY);
+        cp(TW_KZ, tw.kz.tw, NZ);
+        cp(TW_KZL, tw.kz.lo, NZ);
+    }
+    // the same tables as kernel arguments pointing into TW (the dipolar
+    // remainders are not used: those transforms apply plain twiddles)
+    static __device__ __forceinline__ YZTwid shared_twiddles(const C *TW, const YZTwid &tw) {
+        YZTwid t = tw;
+        t.dy.tw  = TW + TW_DY;
+        t.dz.tw  = TW + TW_DZ;
+        t.ky     = Twid{TW + TW_KY, TW + TW_KYL};
+        t.kz     = Twid{TW + TW_KZ, TW + TW_KZL};
+        return t;
     }
     static constexpr int NT0     = 2 * NY * NZ / 16;
     static constexpr int NT      = NT0 < 128 ? 128 : (NT0 > 512 ? 512 : (NT0 + 31) / 32 * 32);
@@ -350,7 +387,7 @@ template <class R, int NY, int NZ> struct YZShape {
 };
 
 // The dipolar chain of a plane, run by NTG threads of barrier group BAR.
-template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
+template <class R, int NY, int NZ, int NTG, int BAR, bool TWS = false> struct DipolarPlane {
     using C         = cplx<R>;
     using G         = YZShape<R, NY, NZ>;
     static constexpr int PS = G::PS, FS = G::FS, NP = G::NP, LD = G::LD, TD = G::TD;
@@ -364,7 +401,7 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
     template <bool WRITE_PHI>
     static __device__ __forceinline__ void inverse(const C *S_g, C *SP, C *DP, R *FP, R *phi_g, R cdd,
                                                    const YZTwid &tw, int t) {
-        using DYI = PlanePass<+1, R, 2 * NY, NZ, 1, PS, NTG, false, true, false, true, BAR>;
+        using DYI = PlanePass<+1, R, 2 * NY, NZ, 1, PS, NTG, false, true, false, true, BAR, TWS>;
         {
             auto lds = [&](int b, int r) { return S_g[r * NZ + b]; };
             typename DYI::First::Regs a0;
@@ -395,8 +432,8 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
             DP[p + m * TD] = z;
         }
         group_sync<BAR, NTG>();
-        PlanePass<+1, R, LD, NP, 1, TD, NTG, false, true, false, true, BAR>::run(DP, (const C *)tw.dz.tw,
-                                                                                (const C *)tw.dz.lo, t);
+        PlanePass<+1, R, LD, NP, 1, TD, NTG, false, true, false, true, BAR, TWS>::run(
+            DP, (const C *)tw.dz.tw, (const C *)tw.dz.lo, t);
         for (int e = t; e < NY * NZ; e += NTG) {
             const int r = e / NZ, k = e - r * NZ;
             const C zz  = DP[(r >> 1) + k * TD];
@@ -407,30 +444,41 @@ template <class R, int NY, int NZ, int NTG, int BAR> struct DipolarPlane {
         }
     }
 
+    // Row pair p of rho (FP): element m of its complex line (m < nz; the upper
+    // half of the zero-padded line is zero and never read).  Consecutive p at
+    // the odd stride FS: distinct banks.
+    static __device__ __forceinline__ C rho_pair(const R *FP, int p, int m) {
+        return C{FP[G::fpi(2 * p, m)], FP[G::fpi(2 * p + 1, m)]};
+    }
+    // Row r, bin m (1 <= m <= nz) of the real transform of rho, unpacked from
+    // the spectrum Z of its row pair in DP: (Z_m + conj(Z_{L-m}))/2 for the even
+    // row, (Z_m - conj(Z_{L-m}))/(2i) for the odd one.  Consecutive m at the odd
+    // stride TD: distinct banks.
+    static __device__ __forceinline__ C rho_bin(const C *DP, int r, int m) {
+        const int p = r >> 1;
+        const C zm  = DP[p + m * TD];
+        const C zc  = DP[p + (LD - m) * TD];
+        if ((r & 1) == 0)
+            return C{(R)0.5 * (zm.x + zc.x), (R)0.5 * (zm.y - zc.y)};
+        return C{(R)0.5 * (zm.y + zc.y), (R)0.5 * (zc.x - zm.x)};
+    }
+
     // rho (FP) -> R2C_z of the row pairs -> FFT_y(2ny, upper half zero) -> S (global).
     // FP must be complete (caller synchronised).
     static __device__ __forceinline__ void forward(C *SP, C *DP, const R *FP, C *S_g, const YZTwid &tw, int t) {
         for (int e = t; e < NP * NZ; e += NTG) {
             const int m = e % NZ, p = e / NZ;
-            DP[p + m * TD] = C{FP[G::fpi(2 * p, m)], FP[G::fpi(2 * p + 1, m)]};
+            DP[p + m * TD] = rho_pair(FP, p, m);
         }
         group_sync<BAR, NTG>();
-        PlanePass<-1, R, LD, NP, 1, TD, NTG, false, false, true, false, BAR>::run(DP, (const C *)tw.dz.tw,
-                                                                                 (const C *)tw.dz.lo, t);
+        PlanePass<-1, R, LD, NP, 1, TD, NTG, false, false, true, false, BAR, TWS>::run(
+            DP, (const C *)tw.dz.tw, (const C *)tw.dz.lo, t);
         for (int e = t; e < NY * NZ; e += NTG) {
             const int r = e / NZ, m = e - r * NZ + 1; // bins 1..nz
-            const int p = r >> 1;
-            const C zm  = DP[p + m * TD];
-            const C zc  = DP[p + (LD - m) * TD];
-            C x;
-            if ((r & 1) == 0)
-                x = C{(R)0.5 * (zm.x + zc.x), (R)0.5 * (zm.y - zc.y)}; // (Z_m + conj(Z_{L-m}))/2
-            else
-                x = C{(R)0.5 * (zm.y + zc.y), (R)0.5 * (zc.x - zm.x)}; // (Z_m - conj(Z_{L-m}))/(2i)
-            SP[r * PS + m - 1] = x;
+            SP[r * PS + m - 1] = rho_bin(DP, r, m);
         }
         group_sync<BAR, NTG>();
-        PlanePass<-1, R, 2 * NY, NZ, 1, PS, NTG, false, false, true, false, BAR>::run_emit(
+        PlanePass<-1, R, 2 * NY, NZ, 1, PS, NTG, false, false, true, false, BAR, TWS>::run_emit(
             SP, [&](int b, int r, C v) { S_g[r * NZ + b] = v; }, (const C *)tw.dy.tw, (const C *)tw.dy.lo, t);
     }
 };
@@ -473,6 +521,12 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
     constexpr bool RT_DIRECT = RT && HAS_INV;
     constexpr bool IT_BULK   = MODE == ZM_IT_MID; // the stencil's planes by bulk copies
     __shared__ __align__(8) unsigned long long pbar;
+    // twiddle tables first (cp.async group 0): they land long before the
+    // first stage's plane loads, and no stage waits for L2 on a twiddle
+    C *TW = reinterpret_cast<C *>(g_smem + G::template smem_base<MODE>());
+    if (RT)
+        G::twiddles_in(TW, tw, tid, NT);
+    const YZTwid tws = RT ? G::shared_twiddles(TW, tw) : tw;
     cp_async_commit();
     if (RT && !RT_DIRECT)
         plane_in_async<C, NY, NZ, PS, NT>(PP, reinterpret_cast<const C *>(a.psi_in) + (size_t)i * NY * NZ, tid);
@@ -515,22 +569,22 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
         // The dipolar and the kinetic transforms run stage by stage side by side
         // (joint_stages); they meet for phi before the phase and rho after it.
         constexpr int NP = G::NP, LD = G::LD, TD = G::TD;
-        using DYI = PlanePass<+1, R, 2 * NY, NZ, 1, PS, NT, false, true, false, true>;
-        using KYI = PlanePass<+1, R, NY, NZ, 1, PS, NT, true, false>;
-        using C2R = PlanePass<+1, R, LD, NP, 1, TD, NT, false, true, false, true>;
-        using ZI  = PlanePass<+1, R, NZ, NY, PS, 1, NT, true, false>;
-        using ZF  = PlanePass<-1, R, NZ, NY, PS, 1, NT, true, true>;
-        using R2C = PlanePass<-1, R, LD, NP, 1, TD, NT, false, false, true, false>;
-        using KYF = PlanePass<-1, R, NY, NZ, 1, PS, NT, true, false>;
-        using DYF = PlanePass<-1, R, 2 * NY, NZ, 1, PS, NT, false, false, true, false>;
+        using DYI = PlanePass<+1, R, 2 * NY, NZ, 1, PS, NT, false, true, false, true, 0, true>;
+        using KYI = PlanePass<+1, R, NY, NZ, 1, PS, NT, true, false, false, false, 0, true>;
+        using C2R = PlanePass<+1, R, LD, NP, 1, TD, NT, false, true, false, true, 0, true>;
+        using ZI  = PlanePass<+1, R, NZ, NY, PS, 1, NT, true, false, false, false, 0, true>;
+        using ZF  = PlanePass<-1, R, NZ, NY, PS, 1, NT, true, true, false, false, 0, true>;
+        using R2C = PlanePass<-1, R, LD, NP, 1, TD, NT, false, false, true, false, 0, true>;
+        using KYF = PlanePass<-1, R, NY, NZ, 1, PS, NT, true, false, false, false, 0, true>;
+        using DYF = PlanePass<-1, R, 2 * NY, NZ, 1, PS, NT, false, false, true, false, 0, true>;
         static_assert(ZI::Last::RADIX == ZF::First::RADIX && ZI::Last::ROUNDS == ZF::First::ROUNDS &&
                           ZI::Last::ITEMS == ZF::First::ITEMS,
                       "paired z transforms share the register layout");
         static_assert(KYF::NSTG >= 2 && DYF::NSTG >= 2, "y lines of at least two stages");
-        const C *dyt = (const C *)tw.dy.tw, *dyl = (const C *)tw.dy.lo;
-        const C *dzt = (const C *)tw.dz.tw, *dzl = (const C *)tw.dz.lo;
-        const C *kyt = (const C *)tw.ky.tw, *kyl = (const C *)tw.ky.lo;
-        const C *kzt = (const C *)tw.kz.tw, *kzl = (const C *)tw.kz.lo;
+        const C *dyt = (const C *)tws.dy.tw, *dyl = (const C *)tws.dy.lo;
+        const C *dzt = (const C *)tws.dz.tw, *dzl = (const C *)tws.dz.lo;
+        const C *kyt = (const C *)tws.ky.tw, *kyl = (const C *)tws.ky.lo;
+        const C *kzt = (const C *)tws.kz.tw, *kzl = (const C *)tws.kz.lo;
         constexpr bool WRITE_PHI = MODE != ZM_RT_MID; // read only after the last iteration
         typename ZI::Last::Regs zr;
         if (HAS_INV) {
@@ -547,6 +601,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
                 KYI::First::read_ld(ldq, ka0, tid);
                 DYI::First::write(SP, da0, tid);
                 KYI::First::write(PP, ka0, tid);
+                cp_async_wait<2>(); // the twiddles (V and the kept psi may still be in flight)
                 __syncthreads();
             }
             joint_stages<DYI, 1, DYI::NSTG, KYI, 1, KYI::NSTG>(SP, dyt, dyl, PP, kyt, kyl, tid);
@@ -676,17 +731,19 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
         }
         __syncthreads(); // rho complete
 
-        // R2C pair lines from rho (upper half zero) || kinetic FFT_z
-        for (int e = tid; e < NP * NZ; e += NT) {
-            const int m = e % NZ, p = e / NZ;
-            DP[p + m * TD] = C{FP[G::fpi(2 * p, m)], FP[G::fpi(2 * p + 1, m)]};
-        }
+        using DW = DipolarPlane<R, NY, NZ, NT, 0, true>;
         if (MODE == ZM_RT_PRO) {
+            // R2C pair lines from rho (upper half zero) || kinetic FFT_z
+            for (int e = tid; e < NP * NZ; e += NT) {
+                const int m = e % NZ, p = e / NZ;
+                DP[p + m * TD] = DW::rho_pair(FP, p, m);
+            }
             __syncthreads();
             joint_stages<R2C, 0, R2C::NSTG, ZF, 0, ZF::NSTG>(DP, dzt, dzl, PP, kzt, kzl, tid);
         } else {
             // first FFT_z stage from the registers (the iFFT_z reads of PP are
-            // behind the two barriers above)
+            // behind the two barriers above) || first R2C stage reading the row
+            // pairs of rho from FP (DP, SP's upper half, is free since the C2R)
 #pragma unroll
             for (int rd = 0; rd < ZF::First::ROUNDS; ++rd) {
                 if (!ZF::First::valid(rd * NT + tid))
@@ -694,34 +751,33 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
                 DFT<ZF::First::RADIX, -1, R, true>::run(zr[rd]);
             }
             ZF::First::write(PP, zr, tid);
+            {
+                auto ldr = [&](int p, int m) { return DW::rho_pair(FP, p, m); };
+                typename R2C::First::Regs ra;
+                R2C::First::read_ld(ldr, ra, tid);
+                R2C::First::write(DP, ra, tid);
+            }
             __syncthreads();
             plane_out<R, NY, NZ, PS, NT>(Pr_g, RP, tid); // kept psi for the next iteration
-            joint_stages<R2C, 0, R2C::NSTG, ZF, 1, ZF::NSTG>(DP, dzt, dzl, PP, kzt, kzl, tid);
+            joint_stages<R2C, 1, R2C::NSTG, ZF, 1, ZF::NSTG>(DP, dzt, dzl, PP, kzt, kzl, tid);
         }
-        // R2C unpacking -> SP rows < ny || kinetic FFT_y stage 0
+        // first stages of the forward y transforms: the dipolar one unpacks the
+        // rows' bins from the R2C output in DP || the kinetic one reads PP
         {
             using K0 = typename KYF::template Stage<0>;
             typename K0::Regs ka;
             K0::read(PP, ka, kyt, kyl, tid);
-            for (int e = tid; e < NY * NZ; e += NT) {
-                const int r = e / NZ, m = e - r * NZ + 1; // bins 1..nz
-                const int p = r >> 1;
-                const C zm  = DP[p + m * TD];
-                const C zc  = DP[p + (LD - m) * TD];
-                C x;
-                if ((r & 1) == 0)
-                    x = C{(R)0.5 * (zm.x + zc.x), (R)0.5 * (zm.y - zc.y)}; // (Z_m + conj(Z_{L-m}))/2
-                else
-                    x = C{(R)0.5 * (zm.y + zc.y), (R)0.5 * (zc.x - zm.x)}; // (Z_m - conj(Z_{L-m}))/(2i)
-                SP[r * PS + m - 1] = x;
-            }
-            __syncthreads();
+            typename DYF::First::Regs da;
+            auto ldu = [&](int b, int r) { return DW::rho_bin(DP, r, b + 1); };
+            DYF::First::read_ld(ldu, da, tid);
+            __syncthreads(); // DP (SP's upper half) and PP read by every thread
             K0::write(PP, ka, tid);
+            DYF::First::write(SP, da, tid);
             __syncthreads();
         }
         // dipolar FFT_y (upper half zero) || kinetic FFT_y, the last stages
         // storing straight to global memory
-        joint_stages<DYF, 0, DYF::NSTG - 1, KYF, 1, KYF::NSTG - 1>(SP, dyt, dyl, PP, kyt, kyl, tid);
+        joint_stages<DYF, 1, DYF::NSTG - 1, KYF, 1, KYF::NSTG - 1>(SP, dyt, dyl, PP, kyt, kyl, tid);
         {
             typename DYF::Last::Regs da;
             DYF::Last::read(SP, da, dyt, dyl, tid);

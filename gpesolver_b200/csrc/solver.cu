@@ -953,7 +953,12 @@ template <class R> class Solver final : public SolverBase {
         // keyed by the schedule too: the plane schedule never tunes y_lines, so a
         // four-kernel solver of the same grid must not reuse its untuned value
         static std::map<std::tuple<int, int, int, int, bool>, std::tuple<int, int, int, int>> chosen;
-        const auto key = std::make_tuple(P.device, nx, ny, nz, yz_plane());
+        // the plane decomposition alone, measured also by solvers whose x widths
+        // are fixed: every solver of a grid then runs the same plane kernels (the
+        // one-CTA and two-CTA real-time kernels agree to rounding, not to the bit)
+        static std::map<std::tuple<int, int, int, int>, int> chosen_p;
+        const auto key  = std::make_tuple(P.device, nx, ny, nz, yz_plane());
+        const auto keyp = std::make_tuple(P.device, nx, ny, nz);
         std::lock_guard<std::mutex> lock(mu);
         const auto it = chosen.find(key);
         if (it != chosen.end()) {
@@ -968,6 +973,17 @@ template <class R> class Solver final : public SolverBase {
                 pair_it = (std::get<3>(it->second) & 2) != 0;
             }
             return;
+        }
+        bool measure_p = tune_p;
+        if (tune_p) {
+            const auto ip = chosen_p.find(keyp);
+            if (ip != chosen_p.end()) {
+                pair_rt   = (ip->second & 1) != 0;
+                pair_it   = (ip->second & 2) != 0;
+                measure_p = false;
+                if (fix_x && !tune_y)
+                    return;
+            }
         }
         GPE_CUDA(cudaMemsetAsync(psi.p, 0, sizeof(C) * N, cur));
         GPE_CUDA(cudaMemsetAsync(S2.p, 0, sizeof(C) * S2.n, cur));
@@ -1033,7 +1049,7 @@ template <class R> class Solver final : public SolverBase {
                 }
             }
         }
-        if (tune_p) {
+        if (measure_p) {
             // the plane kernel of the middle iterations: one CTA per x plane
             // (k4_yz) or a two-CTA cluster per plane (k5_yz_pair[_it]), each
             // timed on the zeroed fields with a zero coefficient table; the
@@ -1064,6 +1080,7 @@ template <class R> class Solver final : public SolverBase {
             GPE_CUDA(cudaMemcpyAsync(norm_state.p, one_buf.p, sizeof(double), cudaMemcpyDeviceToDevice, cur));
             set_divisor_one();
             GPE_CUDA(cudaStreamSynchronize(cur));
+            chosen_p[keyp] = (pair_rt ? 1 : 0) | (pair_it ? 2 : 0);
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);

@@ -48,6 +48,21 @@ def test_autotuner_choice_is_reused_per_grid(monkeypatch):
         assert c.x_tiles() == (16, 16)  # no fused x pass in FP64
 
 
+def test_plane_decomposition_is_shared_when_x_tiles_are_fixed(monkeypatch):
+    """Solvers whose x widths are fixed (GPE_X_TILES) still share the plane
+    decomposition measured once per grid, so every solver of a grid runs the
+    same plane kernels (the one-CTA and two-CTA real-time kernels agree to
+    rounding, not to the bit)."""
+    monkeypatch.delenv("GPE_PLANE_PAIR", raising=False)
+    p = gparams(WELL_CONDITIONED(64, 64, 32))
+    picks = []
+    for tiles in ("16,16", "8,8", "16,8", "8,16"):
+        monkeypatch.setenv("GPE_X_TILES", tiles)
+        with G.B200GrossPitaevskiSolver(p) as s:
+            picks.append(s.plane_kernel())
+    assert picks[0] in ("k4_yz", "k5_yz_pair") and len(set(picks)) == 1, picks
+
+
 def test_y_column_choices_give_identical_results(monkeypatch):
     # four-kernel schedule: z columns per CTA of the y lines
     p = gparams(WELL_CONDITIONED(32, 256, 16))
