@@ -350,10 +350,9 @@ template <class R, int NY, int NZ> struct YZShape {
                          TW_KZ = TW_KYL + NY, TW_KZL = TW_KZ + NZ, TWN = TW_KZL + NZ;
     static constexpr size_t TW_B = sizeof(C) * TWN;
     static_assert(SMEM % 8 == 0 && SMEM_RT % 8 == 0 && SMEM_IT % 8 == 0, "8-byte aligned twiddle region");
-    template <int MODE> static constexpr size_t smem() {
-        return smem_base<MODE>() + (MODE <= ZM_RT_EPI ? TW_B : 0);
-    }
-    // cp.async of the tables into TW (real time)
+    template <int MODE> static constexpr size_t smem() { return smem_base<MODE>() + TW_B; }
+    // cp.async of the tables into TW (the kinetic ones only in real time)
+    template <bool KIN>
     static __device__ __forceinline__ void twiddles_in(C *TW, const YZTwid &tw, int tid, int nt) {
         auto cp = [&](int off, const void *src, int n) {
             for (int e = tid; e < n; e += nt)
@@ -361,10 +360,12 @@ template <class R, int NY, int NZ> struct YZShape {
         };
         cp(TW_DY, tw.dy.tw, 2 * NY);
         cp(TW_DZ, tw.dz.tw, LD);
-        cp(TW_KY, tw.ky.tw, NY);
-        cp(TW_KYL, tw.ky.lo, NY);
-        cp(TW_KZ, tw.kz.tw, NZ);
-        cp(TW_KZL, tw.kz.lo, NZ);
+        if (KIN) {
+            cp(TW_KY, tw.ky.tw, NY);
+            cp(TW_KYL, tw.ky.lo, NY);
+            cp(TW_KZ, tw.kz.tw, NZ);
+            cp(TW_KZL, tw.kz.lo, NZ);
+        }
     }
     // the same tables as kernel arguments pointing into TW (the dipolar
     // remainders are not used: those transforms apply plain twiddles)
@@ -464,21 +465,31 @@ template <class R, int NY, int NZ, int NTG, int BAR, bool TWS = false> struct Di
     }
 
     // rho (FP) -> R2C_z of the row pairs -> FFT_y(2ny, upper half zero) -> S (global).
-    // FP must be complete (caller synchronised).
+    // FP must be complete and DP free (caller synchronised).  The first stage of
+    // the R2C reads the row pairs from FP, the first stage of the y transform
+    // unpacks the rows' bins from DP: neither goes through a copy in the tiles.
     static __device__ __forceinline__ void forward(C *SP, C *DP, const R *FP, C *S_g, const YZTwid &tw, int t) {
-        for (int e = t; e < NP * NZ; e += NTG) {
-            const int m = e % NZ, p = e / NZ;
-            DP[p + m * TD] = rho_pair(FP, p, m);
+        using R2C = PlanePass<-1, R, LD, NP, 1, TD, NTG, false, false, true, false, BAR, TWS>;
+        using DYF = PlanePass<-1, R, 2 * NY, NZ, 1, PS, NTG, false, false, true, false, BAR, TWS>;
+        {
+            auto ldr = [&](int p, int m) { return rho_pair(FP, p, m); };
+            typename R2C::First::Regs a0;
+            R2C::First::read_ld(ldr, a0, t);
+            R2C::First::write(DP, a0, t);
+            group_sync<BAR, NTG>();
         }
-        group_sync<BAR, NTG>();
-        PlanePass<-1, R, LD, NP, 1, TD, NTG, false, false, true, false, BAR, TWS>::run(
-            DP, (const C *)tw.dz.tw, (const C *)tw.dz.lo, t);
-        for (int e = t; e < NY * NZ; e += NTG) {
-            const int r = e / NZ, m = e - r * NZ + 1; // bins 1..nz
-            SP[r * PS + m - 1] = rho_bin(DP, r, m);
+        R2C::template stages<1, R2C::NSTG>(DP, (const C *)tw.dz.tw, (const C *)tw.dz.lo, t);
+        {
+            // bins 1..nz of the rows, stored at kz - 1 (line b = kz - 1)
+            auto ldu = [&](int b, int r) { return rho_bin(DP, r, b + 1); };
+            typename DYF::First::Regs a0;
+            DYF::First::read_ld(ldu, a0, t);
+            group_sync<BAR, NTG>(); // DP (SP's upper half) read by every thread
+            DYF::First::write(SP, a0, t);
+            group_sync<BAR, NTG>();
         }
-        group_sync<BAR, NTG>();
-        PlanePass<-1, R, 2 * NY, NZ, 1, PS, NTG, false, false, true, false, BAR, TWS>::run_emit(
+        static_assert(DYF::NSTG >= 2, "y lines of at least two stages");
+        DYF::template run_emit<1>(
             SP, [&](int b, int r, C v) { S_g[r * NZ + b] = v; }, (const C *)tw.dy.tw, (const C *)tw.dy.lo, t);
     }
 };
@@ -524,9 +535,8 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
     // twiddle tables first (cp.async group 0): they land long before the
     // first stage's plane loads, and no stage waits for L2 on a twiddle
     C *TW = reinterpret_cast<C *>(g_smem + G::template smem_base<MODE>());
-    if (RT)
-        G::twiddles_in(TW, tw, tid, NT);
-    const YZTwid tws = RT ? G::shared_twiddles(TW, tw) : tw;
+    G::template twiddles_in<RT>(TW, tw, tid, NT);
+    const YZTwid tws = G::shared_twiddles(TW, tw);
     cp_async_commit();
     if (RT && !RT_DIRECT)
         plane_in_async<C, NY, NZ, PS, NT>(PP, reinterpret_cast<const C *>(a.psi_in) + (size_t)i * NY * NZ, tid);
@@ -805,7 +815,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
             }
         }
     } else {
-        using DW = DipolarPlane<R, NY, NZ, NT, 0>;
+        using DW = DipolarPlane<R, NY, NZ, NT, 0, true>;
         // imaginary time: psi_in / sqrt(divisor)
         const C *__restrict__ pin = reinterpret_cast<const C *>(a.psi_in);
         C *__restrict__ pout      = reinterpret_cast<C *>(a.psi_out);
@@ -822,7 +832,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
                 FP[G::fpi(r, k)] = wat * (p.x * p.x + p.y * p.y);
             }
         } else {
-            DW::template inverse<true>(S_g, SP, DP, FP, phi_g, cdd, tw, tid);
+            DW::template inverse<true>(S_g, SP, DP, FP, phi_g, cdd, tws, tid);
             __syncthreads(); // FP complete
             const StepCoef cf = a.step.coef[0];
             const R g3w = (R)cf.g3w, gw15 = (R)cf.gw15;
@@ -863,7 +873,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
             }
         }
         __syncthreads(); // rho complete; SP's upper half (DP) free
-        DW::forward(SP, DP, FP, S_g, tw, tid);
+        DW::forward(SP, DP, FP, S_g, tws, tid);
 
         // ---- norm of psi' (imaginary time): deterministic two-level reduction -----
         if (MODE == ZM_IT_MID) {
