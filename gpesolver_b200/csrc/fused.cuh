@@ -139,18 +139,20 @@ __global__ void __launch_bounds__(NT)
     const int cols = ny * nz;
     const int c0   = blockIdx.x * CNT;
     const int cnt  = min(CNT, cols - c0);
+    // the line's (1+wy)(1+wz) - 1, read before the transform so that its L2
+    // reads land behind the line loads
+    const int b = Fw::line_of(tid);
+    C wyz       = C{(R)0, (R)0};
+    if (b < cnt) {
+        const int c = c0 + b, j = c / nz, k = c - j * nz;
+        const C wy = __ldg(&ey[j]), wz = __ldg(&ez[k]);
+        wyz        = cadd(cadd(wy, wz), cmul(wy, wz));
+    }
     C a[Fw::ROUNDSL][Fw::RL];
     Fw::run_to_regs(
         buf, [&](int b, int t) { return b < cnt ? psi[(size_t)t * cols + c0 + b] : C{(R)0, (R)0}; }, a, tw, tl,
         tid);
     {
-        const int b = Fw::line_of(tid);
-        C wyz       = C{(R)0, (R)0};
-        if (b < cnt) {
-            const int c = c0 + b, j = c / nz, k = c - j * nz;
-            const C wy = __ldg(&ey[j]), wz = __ldg(&ez[k]);
-            wyz        = cadd(cadd(wy, wz), cmul(wy, wz)); // (1+wy)(1+wz) - 1
-        }
 #pragma unroll
         for (int rd = 0; rd < Fw::ROUNDSL; ++rd) {
             if (!Fw::template valid<Fw::ITEMSL>(rd * NT + tid))
@@ -217,6 +219,9 @@ __global__ void __launch_bounds__(NT, NX >= 256 ? 2 : 3) // 512-point lines: two
         cp_async4(&vs[e], &vk[(size_t)ix * xs + (size_t)iy * nz + kz]);
     }
     cp_async_commit();
+    // the spectrum's scale (imaginary time: over the norm of the psi it was
+    // built from), read before the transform
+    const R scale = (R)(divisor ? dip_scale / divisor[0] : dip_scale);
     auto ld = [&](int b, int t) { return b < cnt ? S[(size_t)t * cols + c0 + b] : C{(R)0, (R)0}; };
     C a[Fw::ROUNDSL][Fw::RL];
     Fw::stage0_to_tile(buf, ld, tid);
@@ -232,7 +237,6 @@ __global__ void __launch_bounds__(NT, NX >= 256 ? 2 : 3) // 512-point lines: two
         Fw::loadL(buf, a[rd], j, b, twu, nullptr);
     }
     {
-        const R scale = (R)(divisor ? dip_scale / divisor[0] : dip_scale);
         const int b   = Fw::line_of(tid);
 #pragma unroll
         for (int rd = 0; rd < Fw::ROUNDSL; ++rd) {

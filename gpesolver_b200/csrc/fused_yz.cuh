@@ -522,6 +522,41 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
     C *Pr_g        = reinterpret_cast<C *>(a.psi_r) + (size_t)i * NY * NZ;
     const R cdd    = (R)a.cdd;
 
+    // The step coefficients, read first: the chunk counter and the table entry
+    // it selects are two dependent L2 reads, which land behind the plane loads
+    // instead of stalling every warp at the phase step (real time: the sum of
+    // this iteration's and the next one's half steps in the middle iterations;
+    // imaginary time: the table's first entry).
+    R g3 = (R)0, gw = (R)0;
+    {
+        const StepCoef c0 = a.step.coef[RT ? *a.step.base + a.step.local : 0];
+        if (MODE == ZM_RT_MID) {
+            const StepCoef c1 = a.step.coef[*a.step.base + a.step.local + 1];
+            g3                = (R)(c0.g3w + c1.g3w);
+            gw                = (R)(c0.gw15 + c1.gw15);
+        } else {
+            g3 = (R)c0.g3w;
+            gw = (R)c0.gw15;
+        }
+    }
+
+    // Imaginary time: the kept boundary values of this thread's stencil points,
+    // also read at kernel start (every row has its two z-boundary points, so
+    // read at the stencil step they would hold every warp for an L2 round trip)
+    constexpr int SE = (NY * NZ + NT - 1) / NT; // stencil points per thread
+    C bpre[MODE == ZM_IT_MID ? SE : 1];
+    if constexpr (MODE == ZM_IT_MID) {
+        const C *bp     = reinterpret_cast<const C *>(a.bnd) + (size_t)i * NY * NZ;
+        const bool xin0 = i >= 1 && i < nx - 1;
+#pragma unroll
+        for (int j = 0; j < SE; ++j) {
+            const int e = tid + j * NT;
+            const int r = e / NZ, k = e - r * NZ;
+            if (e < NY * NZ && (!xin0 || r < 1 || r >= NY - 1 || k < 1 || k >= NZ - 1))
+                bpre[j] = __ldg(&bp[e]);
+        }
+    }
+
     // ---- load the planes (cp.async groups: none; psi and V; kept real-space psi) ---
     // In real time with the inverse transforms (middle and last iterations) the
     // first stages of the inverse y transforms read the S and psi planes from
@@ -677,21 +712,8 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
         __syncthreads(); // FP = V + cdd phi
 
         // merged potential half steps: theta = -dt/2 [cV (V + cdd phi) + g3 |psi|^2 + gw |psi|^3]
-        R cV, g3, gw;
-        {
-            const int base    = *a.step.base + a.step.local;
-            const StepCoef c0 = a.step.coef[base];
-            if (MODE == ZM_RT_MID) {
-                const StepCoef c1 = a.step.coef[base + 1];
-                cV                = (R)2;
-                g3                = (R)(c0.g3w + c1.g3w);
-                gw                = (R)(c0.gw15 + c1.gw15);
-            } else {
-                cV = (R)1;
-                g3 = (R)c0.g3w;
-                gw = (R)c0.gw15;
-            }
-        }
+        // (g3, gw: the step coefficients loaded at kernel start)
+        const R cV = MODE == ZM_RT_MID ? (R)2 : (R)1;
         const R hdt = (R)a.half_dt, wat = (R)a.w_atoms;
         const bool xin = i >= 1 && i < nx - 1;
         auto phase = [&](C p, int y, int z) -> C {
@@ -819,7 +841,6 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
         // imaginary time: psi_in / sqrt(divisor)
         const C *__restrict__ pin = reinterpret_cast<const C *>(a.psi_in);
         C *__restrict__ pout      = reinterpret_cast<C *>(a.psi_out);
-        const C *__restrict__ bnd = reinterpret_cast<const C *>(a.bnd);
         const R sc        = (R)(1.0 / sqrt(a.norm_state[1]));
         const R wat       = (R)a.w_atoms;
         const size_t pln  = (size_t)NY * NZ;
@@ -834,8 +855,7 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
         } else {
             DW::template inverse<true>(S_g, SP, DP, FP, phi_g, cdd, tws, tid);
             __syncthreads(); // FP complete
-            const StepCoef cf = a.step.coef[0];
-            const R g3w = (R)cf.g3w, gw15 = (R)cf.gw15;
+            const R g3w = g3, gw15 = gw; // a.step.coef[0], loaded at kernel start
             const R cx = (R)a.cx, cy = (R)a.cy, cz = (R)a.cz, dtau = (R)a.dtau;
             const bool xin = i >= 1 && i < nx - 1;
             // the three planes (bulk copies issued at kernel start); a copy that
@@ -844,13 +864,16 @@ __global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz
                 a.status[1] = 1;
                 mbar_wait(&pbar, 0, 1 << 22);
             }
-#pragma unroll 2
-            for (int e = tid; e < NY * NZ; e += NT) {
+#pragma unroll
+            for (int j = 0; j < SE; ++j) {
+                const int e = tid + j * NT;
+                if (SE * NT != NY * NZ && e >= NY * NZ)
+                    break;
                 const int r = e / NZ, k = e - r * NZ;
                 const size_t q = base + e;
                 C o;
                 if (!xin || r < 1 || r >= NY - 1 || k < 1 || k >= NZ - 1) {
-                    o = __ldg(&bnd[q]);
+                    o = bpre[j]; // bnd[q], read at kernel start
                 } else {
                     const C *pp = PP + e; // this plane and its x neighbours (unpadded)
                     const C c0 = cscale(pp[0], sc);

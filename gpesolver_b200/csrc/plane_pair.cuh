@@ -168,6 +168,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairShape<R, NY, NZ>
     const C *dzt = (const C *)tw.dz.tw, *dzl = (const C *)tw.dz.lo;
     const C *kyt = (const C *)tw.ky.tw, *kyl = (const C *)tw.ky.lo;
     const C *kzt = (const C *)tw.kz.tw, *kzl = (const C *)tw.kz.lo;
+    // the step coefficients of this and the next iteration, read first (two
+    // dependent L2 reads that land behind the plane loads)
+    R g3, gw;
+    {
+        const int base     = *a.step.base + a.step.local;
+        const StepCoef c0c = a.step.coef[base];
+        const StepCoef c1c = a.step.coef[base + 1];
+        g3                 = (R)(c0c.g3w + c1c.g3w);
+        gw                 = (R)(c0c.gw15 + c1c.gw15);
+    }
 
     // ---- loads: the column halves of both spectra; V and the kept psi of this
     // CTA's rows (needed from the C2R's last stage on) ----------------------
@@ -270,14 +280,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairShape<R, NY, NZ>
 
     // merged potential half steps of two consecutive iterations:
     // theta = -dt/2 [2 (V + cdd phi) + g3 |psi|^2 + gw |psi|^3]
-    R g3, gw;
-    {
-        const int base     = *a.step.base + a.step.local;
-        const StepCoef c0c = a.step.coef[base];
-        const StepCoef c1c = a.step.coef[base + 1];
-        g3                 = (R)(c0c.g3w + c1c.g3w);
-        gw                 = (R)(c0c.gw15 + c1c.gw15);
-    }
     const R cV = (R)2, hdt = (R)a.half_dt, wat = (R)a.w_atoms;
     const bool xin = i >= 1 && i < nx - 1;
 #pragma unroll
@@ -459,6 +461,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairShape<R, NY, NZ>
     const bool xin   = i >= 1 && i < nx - 1;
     const C *dyt = (const C *)tw.dy.tw, *dyl = (const C *)tw.dy.lo;
     const C *dzt = (const C *)tw.dz.tw, *dzl = (const C *)tw.dz.lo;
+    // the stencil's step coefficients and the kept boundary values of this
+    // thread's stencil points, read first (behind the plane loads; every row
+    // has its two z-boundary points)
+    const StepCoef cf = a.step.coef[0];
+    constexpr int SE  = (NYH * NZ + NT - 1) / NT; // stencil points per thread
+    C bpre[SE];
+#pragma unroll
+    for (int j = 0; j < SE; ++j) {
+        const int e = tid + j * NT;
+        const int rl = e / NZ, k = e - rl * NZ, y = y0 + rl;
+        if (e < NYH * NZ && (!xin || y < 1 || y >= NY - 1 || k < 1 || k >= NZ - 1))
+            bpre[j] = __ldg(&bnd[pl + (size_t)y * NZ + k]);
+    }
 
     // ---- loads: the dipolar column half; V, the psi rows of the stencil ------
 #pragma unroll 4
@@ -555,17 +570,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairShape<R, NY, NZ>
         // elsewhere
         const R sc        = (R)(1.0 / sqrt(a.norm_state[1]));
         const R wat       = (R)a.w_atoms;
-        const StepCoef cf = a.step.coef[0];
         const R g3w = (R)cf.g3w, gw15 = (R)cf.gw15;
         const R cx = (R)a.cx, cy = (R)a.cy, cz = (R)a.cz, dtau = (R)a.dtau;
-#pragma unroll 2
-        for (int e = tid; e < NYH * NZ; e += NT) {
+#pragma unroll
+        for (int j = 0; j < SE; ++j) {
+            const int e = tid + j * NT;
+            if (SE * NT != NYH * NZ && e >= NYH * NZ)
+                break;
             const int rl   = e / NZ, k = e - rl * NZ;
             const int y    = y0 + rl;
             const size_t q = pl + (size_t)y * NZ + k;
             C o;
             if (!xin || y < 1 || y >= NY - 1 || k < 1 || k >= NZ - 1) {
-                o = __ldg(&bnd[q]);
+                o = bpre[j]; // bnd[q], read at kernel start
             } else {
                 const C *pp = PH + (rl + 1) * PZ + k;
                 const C c0v = cscale(pp[0], sc);
