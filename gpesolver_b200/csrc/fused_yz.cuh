@@ -382,8 +382,11 @@ template <class R, int NY, int NZ> struct YZShape {
     // Threads of the kernel in each mode: the imaginary-time modes (62-80
     // registers, no kinetic chain; latency bound on their plane loads) run twice
     // the real-time count, at most 1024.
-    template <int MODE> static constexpr int nt() {
-        return (MODE == ZM_IT_PRO || MODE == ZM_IT_MID) ? (2 * NT > 1024 ? 1024 : 2 * NT) : NT;
+    // WIDE = false keeps the real-time count in imaginary time too: the
+    // autotuner picks per grid (the wide block wins at 64^2 x 16, the narrow
+    // one at 128^2 x 32)
+    template <int MODE, bool WIDE = true> static constexpr int nt() {
+        return (WIDE && (MODE == ZM_IT_PRO || MODE == ZM_IT_MID)) ? (2 * NT > 1024 ? 1024 : 2 * NT) : NT;
     }
 };
 
@@ -494,11 +497,11 @@ template <class R, int NY, int NZ, int NTG, int BAR, bool TWS = false> struct Di
     }
 };
 
-template <class R, int NY, int NZ, int MODE>
-__global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE>()) k4_yz(ZArgs a, YZTwid tw) {
+template <class R, int NY, int NZ, int MODE, bool WIDE = true>
+__global__ void __launch_bounds__(YZShape<R, NY, NZ>::template nt<MODE, WIDE>()) k4_yz(ZArgs a, YZTwid tw) {
     using C                = cplx<R>;
     using G                = YZShape<R, NY, NZ>;
-    constexpr int NT       = G::template nt<MODE>();
+    constexpr int NT       = G::template nt<MODE, WIDE>();
     constexpr int PS       = G::PS;
     constexpr bool RT      = MODE <= ZM_RT_EPI;
     constexpr bool HAS_INV = (MODE == ZM_RT_MID || MODE == ZM_RT_EPI || MODE == ZM_IT_MID);

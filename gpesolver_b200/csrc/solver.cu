@@ -857,6 +857,7 @@ template <class R> class Solver final : public SolverBase {
         set((const void *)k4_yz<R, A, B, ZM_RT_EPI>, G::template smem<ZM_RT_EPI>());               \
         set((const void *)k4_yz<R, A, B, ZM_IT_PRO>, G::template smem<ZM_IT_PRO>());               \
         set((const void *)k4_yz<R, A, B, ZM_IT_MID>, G::template smem<ZM_IT_MID>());               \
+        set((const void *)k4_yz<R, A, B, ZM_IT_MID, false>, G::template smem<ZM_IT_MID>());        \
         set((const void *)k5_yz_pair<R, A, B>, PairShape<R, A, B>::SMEM);                          \
         set((const void *)k5_yz_pair_it<R, A, B>, PairShapeIT<R, A, B>::SMEM);                     \
     }
@@ -930,6 +931,14 @@ template <class R> class Solver final : public SolverBase {
                 fix_p             = true;
             }
         }
+        // GPE_IT_WIDE=0|1 fixes the one-CTA imaginary-time kernel's block
+        bool fix_w = false;
+        if (const char *env = std::getenv("GPE_IT_WIDE")) {
+            if (env[0] == '0' || env[0] == '1') {
+                it_wide = env[0] == '1';
+                fix_w   = true;
+            }
+        }
         const bool tune_p = yz_plane() && !fix_p;
         if (const char *env = std::getenv("GPE_X_TILES")) {
             int k = 0, d = 0;
@@ -971,6 +980,8 @@ template <class R> class Solver final : public SolverBase {
             if (tune_p) {
                 pair_rt = (std::get<3>(it->second) & 1) != 0;
                 pair_it = (std::get<3>(it->second) & 2) != 0;
+                if (!fix_w)
+                    it_wide = (std::get<3>(it->second) & 4) == 0;
             }
             return;
         }
@@ -980,6 +991,8 @@ template <class R> class Solver final : public SolverBase {
             if (ip != chosen_p.end()) {
                 pair_rt   = (ip->second & 1) != 0;
                 pair_it   = (ip->second & 2) != 0;
+                if (!fix_w)
+                    it_wide = (ip->second & 4) == 0;
                 measure_p = false;
                 if (fix_x && !tune_y)
                     return;
@@ -1058,6 +1071,16 @@ template <class R> class Solver final : public SolverBase {
             tcoef.alloc(2);
             GPE_CUDA(cudaMemsetAsync(tcoef.p, 0, sizeof(StepCoef) * 2, cur));
             GPE_CUDA(cudaMemsetAsync(iter_base.p, 0, sizeof(int), cur));
+            // the one-CTA imaginary-time kernel's block: twice the real-time
+            // count or the real-time count (narrow only when 3% faster)
+            pair_rt = pair_it = false;
+            if (!fix_w) {
+                it_wide         = true;
+                const float tw_ = time_of([&] { f_yz<ZM_IT_MID>(cur, psi.p, psii.p, tcoef.p, 0); });
+                it_wide         = false;
+                const float tn_ = time_of([&] { f_yz<ZM_IT_MID>(cur, psi.p, psii.p, tcoef.p, 0); });
+                it_wide         = !(tn_ < 0.97f * tw_);
+            }
             float trt[2], tit[2];
             for (int v = 0; v < 2; ++v) {
                 pair_rt = pair_it = v == 1;
@@ -1080,15 +1103,17 @@ template <class R> class Solver final : public SolverBase {
             GPE_CUDA(cudaMemcpyAsync(norm_state.p, one_buf.p, sizeof(double), cudaMemcpyDeviceToDevice, cur));
             set_divisor_one();
             GPE_CUDA(cudaStreamSynchronize(cur));
-            chosen_p[keyp] = (pair_rt ? 1 : 0) | (pair_it ? 2 : 0);
+            if (!fix_w) // only measured choices are shared
+                chosen_p[keyp] = (pair_rt ? 1 : 0) | (pair_it ? 2 : 0) | (it_wide ? 0 : 4);
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         xk_lines = best_k;
         xd_lines = best_d;
         y_lines  = best_y;
-        if (!fix_x && !fix_y && !fix_p) // only measured choices are shared
-            chosen[key] = std::make_tuple(best_k, best_d, best_y, (pair_rt ? 1 : 0) | (pair_it ? 2 : 0));
+        if (!fix_x && !fix_y && !fix_p && !fix_w) // only measured choices are shared
+            chosen[key] = std::make_tuple(best_k, best_d, best_y,
+                                          (pair_rt ? 1 : 0) | (pair_it ? 2 : 0) | (it_wide ? 0 : 4));
     }
     void x_tiles(int *k, int *d) const override {
         *k = xk_lines;
@@ -1181,6 +1206,9 @@ template <class R> class Solver final : public SolverBase {
         else if (MODE == ZM_IT_MID && pair_it)                                                     \
             launch(k5_yz_pair_it<R, A, B>, 2 * nx, PairShape<R, A, B>::NT,                         \
                    PairShapeIT<R, A, B>::SMEM, s, a, t);                                           \
+        else if (MODE == ZM_IT_MID && !it_wide)                                                    \
+            launch(k4_yz<R, A, B, ZM_IT_MID, false>, nx, G::template nt<ZM_IT_MID, false>(),       \
+                   G::template smem<ZM_IT_MID>(), s, a, t);                                        \
         else                                                                                       \
             launch(k4_yz<R, A, B, MODE>, nx, G::template nt<MODE>(), G::template smem<MODE>(), s, a, t); \
     }
@@ -1362,6 +1390,9 @@ template <class R> class Solver final : public SolverBase {
     // middle real- / imaginary-time iterations on the two-CTA plane kernels
     // (k5_yz_pair, k5_yz_pair_it) instead of k4_yz: picked by autotune_x
     bool pair_rt = false, pair_it = false;
+    // imaginary-time k4_yz with twice the real-time block (at most 1024
+    // threads) or the real-time block: picked by autotune_x
+    bool it_wide = true;
     DevBuf<C> S2;
     DevBuf<C> psir; // real time: psi in real space after the last phase step
     int xk_lines = 16, xd_lines = 16; // x-pass lines per CTA (autotune_x)

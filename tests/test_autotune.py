@@ -63,6 +63,26 @@ def test_plane_decomposition_is_shared_when_x_tiles_are_fixed(monkeypatch):
     assert picks[0] in ("k4_yz", "k5_yz_pair") and len(set(picks)) == 1, picks
 
 
+def test_imaginary_time_block_widths_agree(monkeypatch):
+    """The one-CTA imaginary-time plane kernel at twice the real-time block and
+    at the real-time block (the autotuner picks per grid; GPE_IT_WIDE fixes
+    it): every butterfly and stencil point is computed alike, only the norm's
+    partial sums are grouped differently."""
+    p = gparams(WELL_CONDITIONED(64, 64, 32))
+    monkeypatch.setenv("GPE_PLANE_PAIR", "0")
+    monkeypatch.setenv("GPE_X_TILES", "16,16")
+    out = {}
+    for wide in ("1", "0"):
+        monkeypatch.setenv("GPE_IT_WIDE", wide)
+        with G.B200GrossPitaevskiSolver(p) as s:
+            s.load_pote(G.potential(p))
+            s.load_buffer(G.initial_psi(p))
+            s.imag_steps(50)
+            out[wide] = (s.export_data().copy(), s.calc_norm())
+    assert rel_l2(out["0"][0], out["1"][0]) < 1e-9
+    assert abs(out["0"][1] - out["1"][1]) < 1e-12 * abs(out["1"][1])
+
+
 def test_y_column_choices_give_identical_results(monkeypatch):
     # four-kernel schedule: z columns per CTA of the y lines
     p = gparams(WELL_CONDITIONED(32, 256, 16))
