@@ -1076,11 +1076,18 @@ template <class R> class Solver final : public SolverBase {
             // agree to 1e-9, and the gap where the narrow block wins is ~2.5%)
             pair_rt = pair_it = false;
             if (!fix_w) {
-                it_wide         = true;
-                const float tw_ = time_of([&] { f_yz<ZM_IT_MID>(cur, psi.p, psii.p, tcoef.p, 0); });
-                it_wide         = false;
-                const float tn_ = time_of([&] { f_yz<ZM_IT_MID>(cur, psi.p, psii.p, tcoef.p, 0); });
-                it_wide         = !(tn_ < 0.99f * tw_);
+                // alternated twice, the faster of each pair kept: the candidates
+                // are a few per cent apart, within a drift of the clocks
+                float tw_ = 0.f, tn_ = 0.f;
+                for (int rep = 0; rep < 2; ++rep) {
+                    it_wide        = true;
+                    const float a_ = time_of([&] { f_yz<ZM_IT_MID>(cur, psi.p, psii.p, tcoef.p, 0); });
+                    it_wide        = false;
+                    const float b_ = time_of([&] { f_yz<ZM_IT_MID>(cur, psi.p, psii.p, tcoef.p, 0); });
+                    tw_            = rep == 0 ? a_ : std::min(tw_, a_);
+                    tn_            = rep == 0 ? b_ : std::min(tn_, b_);
+                }
+                it_wide = !(tn_ < 0.99f * tw_);
             }
             float trt[2], tit[2];
             for (int v = 0; v < 2; ++v) {
