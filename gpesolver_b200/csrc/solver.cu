@@ -1031,22 +1031,21 @@ template <class R> class Solver final : public SolverBase {
         };
         int best_k = xk_lines, best_d = xd_lines, best_y = y_lines;
         if (!fix_x) {
-            float tk = 0.f, td = 0.f;
-            for (int c : {16, 8}) {
-                xk_lines = xd_lines = c;
-                const float a = time_of([&] { f_x(cur, true, nullptr, 1); });
-                const float b = time_of([&] { f_x(cur, false, nullptr, 1); });
-                // 8 lines replace 16 only when 3% faster: choices within the
-                // timing noise stay at the default and do not flip run to run
-                if (c == 16 || a < 0.97f * tk) {
-                    tk     = a;
-                    best_k = c;
-                }
-                if (c == 16 || b < 0.97f * td) {
-                    td     = b;
-                    best_d = c;
+            // each width timed twice, alternated, the faster time of each kept;
+            // 8 lines replace 16 only when 3% faster: choices within the
+            // timing noise stay at the default and do not flip run to run
+            float tk[2] = {0.f, 0.f}, td[2] = {0.f, 0.f}; // [16 lines, 8 lines]
+            for (int rep = 0; rep < 2; ++rep) {
+                for (int v = 0; v < 2; ++v) {
+                    xk_lines = xd_lines = v == 0 ? 16 : 8;
+                    const float a = time_of([&] { f_x(cur, true, nullptr, 1); });
+                    const float b = time_of([&] { f_x(cur, false, nullptr, 1); });
+                    tk[v]         = rep == 0 ? a : std::min(tk[v], a);
+                    td[v]         = rep == 0 ? b : std::min(td[v], b);
                 }
             }
+            best_k = tk[1] < 0.97f * tk[0] ? 8 : 16;
+            best_d = td[1] < 0.97f * td[0] ? 8 : 16;
         }
         if (tune_y) {
             float ty = 0.f;
